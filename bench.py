@@ -1,0 +1,304 @@
+#!/usr/bin/env python
+"""Benchmark of the EAC hot path on B200.
+
+Default workload: Boruvka minimum spanning forest of the 16-nearest-neighbour
+graph of 1,000,000 uniform 3-D points (symmetrised, duplicates merged,
+8,960,895 undirected edges with uint8 weights uniform in [1, 255], int32
+indices).  Metric: MST edges/s = undirected input edges / MST time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1).  The forest does not shard: every
+rank solves its own replica (replicas only, weak scaling) and `value` is the
+edges of all replicas over the slowest rank's time.  `--impl reference` times
+the reference's CPU algorithm (the oracle's C restatement of
+boruvka_minho_seq) on the host cores instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_VERTICES = 1_000_000
+KNN = 16
+SEED = 2
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(n_edges):
+    return {"workload": "boruvka_mst_knn16_1M",
+            "graph": "16-NN of 1,000,000 uniform 3-D points, symmetrised",
+            "n_vertices": N_VERTICES, "undirected_edges": int(n_edges),
+            "directed_entries": int(2 * n_edges), "weights": "uint8 uniform [1,255]",
+            "indices": "int32", "l2": "flushed (256 MiB write) between timed steps"}
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % index)
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.out), exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.out, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index),
+                                          "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.out):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.out) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax.append(float(p[2]))
+                except ValueError:
+                    continue
+                for name, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per contraction launch from the committed ncu summary,
+    scaled to the full workload there (None when no summary exists)."""
+    p = os.path.join(ROOT, "profiles", "boruvka_edge_tile_knn16_1M.md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    return None
+
+
+def cpu_baseline(indptr, dest, w, n_edges, budget_s=12.0):
+    import oracle
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while True:
+        t0 = time.perf_counter()
+        oracle.boruvka_seq(indptr, dest, w)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() > t_end or len(times) >= 10:
+            break
+    t = statistics.median(times)
+    return {"value": n_edges / t, "unit": "edges/s", "cores": 1, "kind": "port",
+            "sample": "full graph, %d runs of the oracle's C restatement of "
+                      "boruvka_minho_seq (single-threaded, like the reference), median" % len(times)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from masters_final_b200 import workloads as W
+    indptr, dest, w = W.knn_graph(N_VERTICES, k=KNN, seed=SEED)
+    n_edges = dest.size // 2
+    import oracle
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle.boruvka_seq(indptr, dest, w)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    tot = sum(times)
+    val = n_edges * len(times) / tot
+    line = {"metric": "MST edges/s", "value": val, "unit": "edges/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * tot / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": workload_config(n_edges),
+            "cpu_baseline": {"value": val, "unit": "edges/s", "cores": 1, "kind": "port",
+                             "sample": "full graph per step; the oracle's C restatement of "
+                                       "boruvka_minho_seq, single-threaded like the reference"},
+            "e2e": {"value": val, "unit": "edges/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from masters_final_b200 import _lib
+    from masters_final_b200 import workloads as W
+    from masters_final_b200.graph.mst import boruvka_minho_gpu
+    import ctypes
+
+    indptr, dest, w = W.knn_graph(N_VERTICES, k=KNN, seed=SEED)
+    n_edges = dest.size // 2
+    first = indptr[:-1].astype(np.int32)
+    deg = np.diff(indptr).astype(np.int32)
+    dev = torch.device("cuda", local)
+    d_dest = torch.from_numpy(dest).to(dev)
+    d_w = torch.from_numpy(w).to(dev)
+    d_first = torch.from_numpy(first).to(dev)
+    d_deg = torch.from_numpy(deg).to(dev)
+    L = _lib.load()
+    V, E = N_VERTICES, dest.size
+    ws = torch.empty(L.eacb_boruvka_workspace_size(V, E), dtype=torch.uint8, device=dev)
+    mst = torch.empty(V, dtype=torch.int32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    nm = ctypes.c_int64(0)
+
+    def step():
+        _lib.check(L.eacb_boruvka_mst(_lib.ptr(d_dest), _lib.ptr(d_w), _lib.U8, _lib.ptr(d_first),
+                                      _lib.ptr(d_deg), V, E, _lib.ptr(mst), ctypes.byref(nm),
+                                      _lib.ptr(ws), ws.numel(), sh), "boruvka")
+
+    def barrier():
+        if world > 1:
+            dist.all_reduce(torch.zeros(1, device=dev))
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    assert nm.value == V - 1
+    # ---- device-resident timed region ----
+    barrier()
+    _lib.profile_enable(True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.fill_(i & 255)
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        barrier()
+    launches, pms, pbytes, pcount = _lib.profile_read()
+    _lib.profile_enable(False)
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    t = torch.tensor([t_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_ms = float(t.item())
+    value = world * n_edges * args.steps / (t_ms / 1000.0)
+
+    # ---- end to end through the public API, host buffers (pinned) ----
+    h_dest = torch.from_numpy(dest).pin_memory()
+    h_w = torch.from_numpy(w).pin_memory()
+    h_first = torch.from_numpy(first).pin_memory()
+    h_deg = torch.from_numpy(deg).pin_memory()
+    boruvka_minho_gpu(h_dest, h_w, h_first, h_deg)      # warm
+    barrier()
+    e_ms = 0.0
+    for i in range(args.steps):
+        flush.fill_(i & 255)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        out, n = boruvka_minho_gpu(h_dest, h_w, h_first, h_deg)
+        b.record(stream)
+        b.synchronize()
+        e_ms += a.elapsed_time(b)
+        assert n == V - 1
+    t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e_ms = float(t.item())
+    e2e = {"value": world * n_edges * args.steps / (e_ms / 1000.0), "unit": "edges/s",
+           "h2d_bytes_per_step": int(dest.nbytes + w.nbytes + first.nbytes + deg.nbytes),
+           "d2h_bytes_per_step": int(4 * (V - 1))}
+
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        achieved = (pbytes[0] / (pms[0] / 1000.0)) / 1e9 if pms[0] > 0 else None
+        traffic = profiled_traffic()
+        roof = {"bound": "hbm", "kernel": "k_edge_tile (Boruvka contraction + fused min-edge)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                "traffic": traffic, "launches": pcount[0],
+                "ms_share_of_step": pms[0] / t_ms if t_ms else None,
+                "algorithmic_bytes": "8 B read per edge word + 8 B written per surviving edge"}
+        line = {"metric": "MST edges/s", "value": value, "unit": "edges/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "u8", "data": "synthetic", "config": workload_config(n_edges),
+                "e2e": e2e, "roofline": roof, "gpu_launches": int(launches),
+                "clocks": clk.summary()}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(indptr, dest, w, n_edges)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,151 @@
+/*
+ * eacb200.h -- C ABI of libeacb200.so, the B200 (sm_100a) evidence
+ * accumulation clustering (EAC) hot path.
+ *
+ * The reference (diogo-aos/masters_final) is Python 2 + Numba and has no
+ * native interface; each entry point below replaces one reference Python
+ * function or kernel sequence, cited as path:line within that project.
+ *
+ * Conventions:
+ *   - every pointer argument is a DEVICE pointer unless the name says host_;
+ *   - `stream` is a cudaStream_t cast to uintptr_t (0 = legacy default stream);
+ *   - scratch memory is a caller-owned device buffer `ws` of `ws_bytes` bytes,
+ *     at least the size returned by the matching *_workspace_size() query,
+ *     256-byte aligned; the library never allocates device memory;
+ *   - functions return an eacb_status (0 = success, negative = error) and
+ *     never throw; outputs are undefined after an error;
+ *   - functions whose work has data-dependent rounds (Boruvka, connected
+ *     components, final clustering) synchronize `stream` once per round to
+ *     read a few counters; all others are asynchronous on `stream`.
+ */
+#ifndef EACB200_H
+#define EACB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    EACB_OK = 0,
+    EACB_ERR_BAD_ARGUMENT = -1,          /* null pointer, negative size, bad enum */
+    EACB_ERR_WORKSPACE = -2,             /* ws too small or an internal capacity exceeded */
+    EACB_ERR_CUDA = -3,                  /* a CUDA runtime call failed */
+    EACB_ERR_UNSUPPORTED = -4,           /* valid input this build does not handle */
+    EACB_ERR_DEVICE_WAIT = -5,           /* a bounded device-side wait gave up */
+    EACB_ERR_NOT_CONVERGED = -6,         /* iteration cap hit (input not a valid graph) */
+    EACB_ERR_FIRST_PARTITION_OVERFLOW = -7, /* reference would write past a row (sparse.py:446-465) */
+    EACB_ERR_BAD_INPUT = -8,             /* input failed a device-side validity check */
+    EACB_ERR_VALUE = -9,                 /* the reference raises ValueError here */
+    EACB_ERR_INTERNAL = -10
+} eacb_status;
+
+/* Element type codes for weight arrays. */
+typedef enum {
+    EACB_U8 = 1,
+    EACB_U16 = 2,
+    EACB_I32 = 3,
+    EACB_U32 = 4,
+    EACB_F32 = 5
+} eacb_dtype;
+
+int eacb_version(void);
+const char *eacb_status_string(int status);
+
+/* Every workspace starts with a device error word that asynchronous entry
+ * points set on a device-side failure.  Synchronizes `stream`, returns the
+ * status that word encodes and clears it. */
+int eacb_workspace_status(void *ws, uintptr_t stream);
+
+/* Built-in profiling, off by default.  eacb_profile_enable(1) resets the
+ * counters and turns on CUDA-event timing (on the launching stream) of the
+ * tagged kernels; eacb_profile_read returns the number of kernels the
+ * library launched since, and per tag (0 = Boruvka contraction tile,
+ * 1 = scan, 2 = co-association rows, 3 = k-means labels; arrays of 8) the
+ * total milliseconds, algorithmic bytes and launches. */
+void eacb_profile_enable(int on);
+void eacb_profile_read(int64_t *launches, double *ms, double *bytes, int64_t *count);
+
+/* ------------------------------------------------------------------------
+ * Exclusive prefix sum.
+ * Replaces MyML/MyML/utils/scan.py:144-249 (scan_gpu, recursive Blelloch
+ * scan) and the CPU scans :42-72 (exprefixsumNumba / exprefixsumNumbaSingle).
+ * out[i] = init + sum(in[0..i)); `in` may equal `out` (in place).  The int32
+ * variant stores each prefix truncated to 32 bits (wraps modulo 2^32 like the
+ * reference's int64 carry stored into an int32 array); *d_total (device int64)
+ * receives the exact 64-bit total.  Single pass (decoupled look-back).
+ * ------------------------------------------------------------------------ */
+size_t eacb_scan_workspace_size(int64_t n);
+int eacb_scan_excl_i32(const int32_t *in, int32_t *out, int64_t n, int64_t init,
+                       int64_t *d_total, void *ws, size_t ws_bytes, uintptr_t stream);
+int eacb_scan_excl_i32_i64(const int32_t *in, int64_t *out, int64_t n, int64_t init,
+                           int64_t *d_total, void *ws, size_t ws_bytes, uintptr_t stream);
+int eacb_scan_excl_i64(const int64_t *in, int64_t *out, int64_t n, int64_t init,
+                       int64_t *d_total, void *ws, size_t ws_bytes, uintptr_t stream);
+
+/* ------------------------------------------------------------------------
+ * Boruvka minimum spanning forest of a symmetric CSR graph.
+ * Replaces MyML/MyML/graph/mst.py:417-564 (boruvka_minho_gpu) and its
+ * kernels :574-809.  Graph: row r has the entries [first_edge[r],
+ * first_edge[r] + out_degree[r]) of dest/weight; every undirected edge is
+ * stored in both directions; self loops are ignored.
+ * Ties are broken by the strict order (weight, min(u,v), max(u,v)), so the
+ * forest is unique.  mst_out (capacity n_vertices - 1) receives, per chosen
+ * edge, the index of its entry in row min(u,v) (the smallest such index with
+ * the chosen weight), in round order, supervertex order within a round;
+ * *host_n_mst receives the number of forest edges.
+ * Requires bits(weight) + 2*ceil(log2(n_vertices)) + 1 <= 64.
+ * ------------------------------------------------------------------------ */
+size_t eacb_boruvka_workspace_size(int32_t n_vertices, int64_t n_edges);
+int eacb_boruvka_mst(const int32_t *dest, const void *weight, int weight_dtype,
+                     const int32_t *first_edge, const int32_t *out_degree,
+                     int32_t n_vertices, int64_t n_edges,
+                     int32_t *mst_out, int64_t *host_n_mst,
+                     void *ws, size_t ws_bytes, uintptr_t stream);
+
+/* ------------------------------------------------------------------------
+ * Connected components by Boruvka contraction, with the reference's own
+ * label numbering: each round a vertex picks its minimum out-edge by
+ * (weight, destination supervertex), the smaller endpoint of a mutual pick
+ * becomes the root, and supervertices are renumbered in root order.
+ * Replaces MyML/MyML/graph/connected_components.py:176-314
+ * (connected_comps_gpu; same labels as connected_comps_seq :46-137).
+ * labels (n_vertices, int32) receive the component labels; *host_n_comps the
+ * number of components.
+ * ------------------------------------------------------------------------ */
+int eacb_connected_components(const int32_t *dest, const void *weight, int weight_dtype,
+                              const int32_t *first_edge, const int32_t *out_degree,
+                              int32_t n_vertices, int64_t n_edges,
+                              int32_t *labels, int64_t *host_n_comps,
+                              void *ws, size_t ws_bytes, uintptr_t stream);
+
+/* ------------------------------------------------------------------------
+ * EAC final clustering of a condensed co-association dissimilarity matrix.
+ * Replaces MyML/MyML/EAC/eac.py:199-267 (sp_sl_lifetime) with
+ * lifetime_n_clusters :366-391, whose MST is the Kruskal of
+ * scipy_numba/scipy_numba/sparse/csgraph/_min_spanning_tree.py:21-175 and
+ * whose labels come from scipy.sparse.csgraph.connected_components.
+ * Input: upper-triangle CSR (row i holds columns j > i, sorted) with uint8
+ * dissimilarities; max_dist = the number of partitions (the reference adds 1).
+ * n_clusters = 0 uses the maximum-lifetime rule.
+ * Outputs: labels (n, int32) numbered by each cluster's smallest member (the
+ * numbering connected_components produces); *host_n_fclusts; *host_labels_valid
+ * = 0 when the reference returns an empty label array (one cluster).
+ * Returns EACB_ERR_VALUE where the reference raises ValueError (fewer than
+ * two MST edges, or no two MST edges of equal weight).
+ * ------------------------------------------------------------------------ */
+size_t eacb_final_clustering_workspace_size(int32_t n, int64_t nnz);
+int eacb_final_clustering(const int64_t *indptr, const int32_t *indices,
+                          const uint8_t *diassoc, int32_t n, int64_t nnz,
+                          int32_t max_dist, int32_t n_clusters,
+                          int32_t *labels, int64_t *host_n_fclusts,
+                          int32_t *host_labels_valid,
+                          void *ws, size_t ws_bytes, uintptr_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EACB200_H */

@@ -1,0 +1,165 @@
+"""ctypes binding of libeacb200.so (the C ABI declared in include/eacb200.h).
+
+PyTorch is used only for device buffers and streams.  There is no fallback:
+if the library or a CUDA device is missing, every entry point raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libeacb200.so")
+
+U8, U16, I32, U32, F32 = 1, 2, 3, 4, 5
+_DTYPE_CODE = {np.dtype(np.uint8): U8, np.dtype(np.uint16): U16, np.dtype(np.int32): I32,
+               np.dtype(np.uint32): U32, np.dtype(np.float32): F32}
+
+ERR_VALUE = -9
+ERR_FIRST_OVERFLOW = -7
+
+_lib = None
+
+class EACBError(RuntimeError):
+    def __init__(self, status, where):
+        self.status = status
+        super().__init__("%s failed: %s (%d)" % (where, status_string(status), status))
+
+
+def load():
+    """Load the library (build it first if this checkout has none)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libeacb200.so is not built; run `python -m masters_final_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    p, i32, i64, sz = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_size_t
+    P64 = ctypes.POINTER(ctypes.c_int64)
+    P32 = ctypes.POINTER(ctypes.c_int32)
+    sigs = {
+        "eacb_version": (ctypes.c_int, []),
+        "eacb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+        "eacb_workspace_status": (ctypes.c_int, [p, p]),
+        "eacb_profile_enable": (None, [ctypes.c_int]),
+        "eacb_profile_read": (None, [p, p, p, p]),
+        "eacb_scan_workspace_size": (sz, [i64]),
+        "eacb_scan_excl_i32": (ctypes.c_int, [p, p, i64, i64, p, p, sz, p]),
+        "eacb_scan_excl_i32_i64": (ctypes.c_int, [p, p, i64, i64, p, p, sz, p]),
+        "eacb_scan_excl_i64": (ctypes.c_int, [p, p, i64, i64, p, p, sz, p]),
+        "eacb_boruvka_workspace_size": (sz, [i32, i64]),
+        "eacb_boruvka_mst": (ctypes.c_int, [p, p, ctypes.c_int, p, p, i32, i64, p, P64, p, sz, p]),
+        "eacb_connected_components": (ctypes.c_int, [p, p, ctypes.c_int, p, p, i32, i64, p, P64,
+                                                     p, sz, p]),
+        "eacb_final_clustering_workspace_size": (sz, [i32, i64]),
+        "eacb_final_clustering": (ctypes.c_int, [p, p, p, i32, i64, i32, i32, p, P64, P32, p, sz,
+                                                 p]),
+    }
+    for name, (res, args) in sigs.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def extend(sigs):
+    """Register more signatures (used by modules that add entry points)."""
+    L = load()
+    for name, (res, args) in sigs.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+
+
+def profile_enable(on=True):
+    load().eacb_profile_enable(1 if on else 0)
+
+
+def profile_read():
+    """(launches, per-tag ms, per-tag algorithmic bytes, per-tag launch counts)."""
+    launches = ctypes.c_int64(0)
+    ms = (ctypes.c_double * 8)()
+    by = (ctypes.c_double * 8)()
+    cnt = (ctypes.c_int64 * 8)()
+    load().eacb_profile_read(ctypes.byref(launches), ms, by, cnt)
+    return int(launches.value), list(ms), list(by), list(cnt)
+
+
+def status_string(s):
+    return load().eacb_status_string(s).decode()
+
+
+def check(status, where):
+    if status != 0:
+        raise EACBError(status, where)
+
+
+def exported_symbols():
+    """Names declared in include/eacb200.h (the C ABI)."""
+    import re
+    hdr = os.path.join(os.path.dirname(_HERE), "include", "eacb200.h")
+    with open(hdr) as f:
+        txt = f.read()
+    decl = r"^(?:const\s+)?\w+\s*\*?\s*(eacb_\w+)\s*\("
+    return sorted(set(re.findall(decl, txt, flags=re.MULTILINE)))
+
+
+# --------------------------------------------------------------- devices ---
+def torch():
+    import torch as _t
+    return _t
+
+
+def device():
+    t = torch()
+    if not t.cuda.is_available():
+        raise RuntimeError("masters_final_b200 needs a CUDA device (B200, sm_100a)")
+    return t.device("cuda", t.cuda.current_device())
+
+
+def stream_handle(stream=None):
+    t = torch()
+    s = stream if stream is not None else t.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def ptr(x):
+    return ctypes.c_void_p(x.data_ptr()) if x is not None else None
+
+
+def workspace(nbytes):
+    t = torch()
+    return t.empty(max(int(nbytes), 256), dtype=t.uint8, device=device())
+
+
+def to_device(a, dtype=None):
+    """numpy array or torch tensor -> contiguous CUDA tensor (no copy if
+    already there with the right dtype)."""
+    t = torch()
+    if isinstance(a, t.Tensor):
+        x = a
+        if dtype is not None:
+            x = x.to(dtype)
+        if not x.is_cuda:
+            x = x.to(device())
+        return x.contiguous()
+    arr = np.ascontiguousarray(a)
+    x = t.from_numpy(arr)
+    if dtype is not None:
+        x = x.to(dtype)
+    return x.to(device(), non_blocking=False).contiguous()
+
+
+def np_dtype_of(x):
+    t = torch()
+    if isinstance(x, t.Tensor):
+        return np.dtype(str(x.dtype).replace("torch.", ""))
+    return np.asarray(x).dtype
+
+
+def dtype_code(x):
+    d = np_dtype_of(x)
+    if d not in _DTYPE_CODE:
+        raise TypeError("unsupported weight dtype %s" % d)
+    return _DTYPE_CODE[d]

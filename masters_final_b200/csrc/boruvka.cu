@@ -1,0 +1,880 @@
+// Boruvka minimum spanning forest, connected components and the EAC final
+// clustering (lifetime cut) on B200.
+//
+// Reference: MyML/MyML/graph/mst.py:417-809 (boruvka_minho_gpu and kernels),
+// MyML/MyML/graph/connected_components.py:176-345, MyML/MyML/EAC/eac.py:199-391.
+//
+// Design (not the reference's):
+//  * Every directed edge is ONE 64-bit word: weight-order bits | min(u,v) |
+//    max(u,v) | direction bit, with u, v the ORIGINAL endpoints.  A round
+//    never rewrites edges; it only drops the ones that became internal.  The
+//    current endpoints are label[u], label[v] (label = original vertex ->
+//    current supervertex, kept for all original vertices, L2 resident).
+//  * Min-edge selection is an atomicMin of a 64-bit selection key per
+//    supervertex: (weight, min, max) for the MST -- a strict total order, so
+//    the forest is unique -- or (weight, destination supervertex) for the
+//    reference's connected-components numbering.  Lanes of a warp holding
+//    edges of the same supervertex are pre-reduced with a segmented shuffle
+//    scan, so one atomic is issued per run, not per edge.
+//  * Contraction is a single-pass, order-preserving stream compaction
+//    (decoupled look-back over 2048-edge tiles) fused with the NEXT round's
+//    min-edge selection: each edge is read once and written once per round.
+//  * Mutual picks are broken towards the larger id like the reference; roots
+//    are found by a bounded pointer chase with path halving; supervertices are
+//    renumbered by an exclusive scan of the root flags (root order), which is
+//    the reference's numbering.
+#include "eacb_common.cuh"
+#include "scan_impl.cuh"
+
+namespace eacb {
+
+enum { SEL_MST = 0, SEL_CC = 1 };
+
+struct Pack {
+    int vbits;
+    int wshift;      // 2*vbits + 1
+    uint64_t vmask;
+    __host__ __device__ uint32_t a(uint64_t k) const { return (uint32_t)((k >> (vbits + 1)) & vmask); }
+    __host__ __device__ uint32_t b(uint64_t k) const { return (uint32_t)((k >> 1) & vmask); }
+    __host__ __device__ uint32_t w(uint64_t k) const { return (uint32_t)(k >> wshift); }
+    __host__ __device__ uint32_t src(uint64_t k) const { return (k & 1) ? b(k) : a(k); }
+    __host__ __device__ uint32_t dst(uint64_t k) const { return (k & 1) ? a(k) : b(k); }
+    __host__ __device__ uint64_t make(uint32_t w, uint32_t u, uint32_t v) const
+    {
+        uint32_t lo = u < v ? u : v, hi = u < v ? v : u;
+        return ((uint64_t)w << wshift) | ((uint64_t)lo << (vbits + 1)) | ((uint64_t)hi << 1) |
+               (uint64_t)(u > v);
+    }
+    // MST selection key (weight, min, max) and its decoding
+    __host__ __device__ uint64_t mst_sel(uint64_t k) const { return k >> 1; }
+    __host__ __device__ uint32_t sel_a(uint64_t s) const { return (uint32_t)((s >> vbits) & vmask); }
+    __host__ __device__ uint32_t sel_b(uint64_t s) const { return (uint32_t)(s & vmask); }
+    __host__ __device__ uint32_t sel_w(uint64_t s) const { return (uint32_t)(s >> (2 * vbits)); }
+};
+
+static int make_pack(int32_t n_vertices, int wbits, Pack &pk)
+{
+    int vbits = 1;
+    while (vbits < 31 && ((int64_t)1 << vbits) < (int64_t)n_vertices) vbits++;
+    if (wbits + 2 * vbits + 1 > 64) return EACB_ERR_UNSUPPORTED;
+    pk.vbits = vbits;
+    pk.wshift = 2 * vbits + 1;
+    pk.vmask = ((uint64_t)1 << vbits) - 1;
+    return EACB_OK;
+}
+
+static int dtype_bits(int dt)
+{
+    switch (dt) {
+    case EACB_U8: return 8;
+    case EACB_U16: return 16;
+    case EACB_I32: case EACB_U32: case EACB_F32: return 32;
+    default: return -1;
+    }
+}
+
+// Order-preserving unsigned image of a weight.
+__device__ __forceinline__ uint32_t wword(uint8_t x) { return x; }
+__device__ __forceinline__ uint32_t wword(uint16_t x) { return x; }
+__device__ __forceinline__ uint32_t wword(uint32_t x) { return x; }
+__device__ __forceinline__ uint32_t wword(int32_t x) { return (uint32_t)x ^ 0x80000000u; }
+__device__ __forceinline__ uint32_t wword(float x)
+{
+    uint32_t u = __float_as_uint(x == 0.0f ? 0.0f : x);   // -0 == +0
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+constexpr uint64_t kNone = ~0ull;
+
+// One atomicMin per run of equal `su` among consecutive lanes.
+__device__ __forceinline__ void seg_min_atomic(bool valid, int32_t su, uint64_t sel,
+                                               unsigned long long *best)
+{
+    const int lane = threadIdx.x & 31;
+    int32_t key = valid ? su : -1 - lane;
+    int32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+    bool head = (lane == 0) || (prev != key);
+    unsigned heads = __ballot_sync(0xffffffffu, head);
+    int start = 31 - __clz(heads & ((2u << lane) - 1u));
+    uint64_t m = valid ? sel : kNone;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint64_t o = __shfl_up_sync(0xffffffffu, m, d);
+        if (lane - d >= start) m = (o < m) ? o : m;
+    }
+    int32_t next = __shfl_down_sync(0xffffffffu, key, 1);
+    bool tail = (lane == 31) || (next != key);
+    if (valid && tail) atomicMin(&best[su], (unsigned long long)m);
+}
+
+constexpr int kET = 256;   // edge-tile threads
+constexpr int kEI = 8;     // edges per thread (striped): 2048 edges per tile
+constexpr int64_t kETile = (int64_t)kET * kEI;
+
+// Edge sources for the tile kernel ------------------------------------------
+// (a) filtering pass over the current edge array
+struct SrcEdges {
+    const uint64_t *e;
+    const int32_t *label;
+    Pack pk;
+    uint32_t V0;
+    __device__ bool load(int64_t i, uint64_t &k, int32_t &su, int32_t &sv, uint32_t &w) const
+    {
+        k = e[i];
+        if (pk.a(k) >= V0 || pk.b(k) >= V0) return false;   // never produced for valid input
+        su = label[pk.src(k)];
+        sv = label[pk.dst(k)];
+        w = pk.w(k);
+        return su != sv;
+    }
+};
+
+// (b) a symmetric CSR (one directed edge per entry); rowid maps entry -> row
+template <typename WT>
+struct SrcCSR {
+    const int32_t *rowid;
+    const int32_t *dest;
+    const WT *weight;
+    int32_t V;
+    Pack pk;
+    int *err;
+    __device__ bool load(int64_t i, uint64_t &k, int32_t &su, int32_t &sv, uint32_t &w) const
+    {
+        int32_t u = rowid[i];
+        if (u < 0) return false;
+        int32_t v = dest[i];
+        if (v < 0 || v >= V) { set_err(err, DEV_BAD_INPUT); return false; }
+        if (u == v) return false;
+        w = wword(weight[i]);
+        k = pk.make(w, (uint32_t)u, (uint32_t)v);
+        su = u;
+        sv = v;
+        return true;
+    }
+};
+
+// (c) both directions of undirected keys (MST selection keys) below a weight cap
+struct SrcForest {
+    const uint64_t *keys;   // selection keys (w, a, b)
+    int64_t n_keys;
+    int64_t wmax;           // keep weights <= wmax (-1 keeps none)
+    Pack pk;
+    __device__ bool load(int64_t i, uint64_t &k, int32_t &su, int32_t &sv, uint32_t &w) const
+    {
+        int64_t j = i < n_keys ? i : i - n_keys;
+        uint64_t s = keys[j];
+        w = pk.sel_w(s);
+        if ((int64_t)w > wmax) return false;
+        uint32_t a = pk.sel_a(s), b = pk.sel_b(s);
+        k = (s << 1) | (uint64_t)(i >= n_keys);
+        su = (int32_t)(i < n_keys ? a : b);
+        sv = (int32_t)(i < n_keys ? b : a);
+        return true;
+    }
+};
+
+// Tile kernel: keep-filter + order-preserving compaction + fused min-edge
+// selection for the next round.
+template <int MODE, typename Src>
+__global__ void __launch_bounds__(kET)
+k_edge_tile(Src src, int64_t n_in, uint64_t *__restrict__ eout, unsigned long long *best,
+            uint64_t *status, int *counter, int64_t *d_count, int *err)
+{
+    __shared__ int s_tile;
+    __shared__ int s_off[kEI][kET / 32];
+    __shared__ int64_t s_prefix;
+    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t base = tile * kETile;
+    uint64_t k[kEI];
+    unsigned bal[kEI];
+#pragma unroll
+    for (int it = 0; it < kEI; ++it) {
+        const int64_t i = base + (int64_t)it * kET + threadIdx.x;
+        int32_t su = 0, sv = 0;
+        uint32_t w = 0;
+        bool keep = false;
+        k[it] = 0;
+        if (i < n_in) keep = src.load(i, k[it], su, sv, w);
+        bal[it] = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) s_off[it][warp] = __popc(bal[it]);
+        uint64_t sel = MODE == SEL_MST ? (k[it] >> 1) : (((uint64_t)w << 32) | (uint32_t)sv);
+        seg_min_atomic(keep, su, sel, best);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        // exclusive scan of the kEI x 8 per-warp counts in (item, warp) order
+        constexpr int N = kEI * (kET / 32);
+        constexpr int PER = N / 32;
+        int c[PER];
+        int sum = 0;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            int idx = lane * PER + q;
+            c[q] = s_off[idx / (kET / 32)][idx % (kET / 32)];
+            sum += c[q];
+        }
+        int incl = sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            int o = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += o;
+        }
+        int run = incl - sum;
+        int tot = __shfl_sync(0xffffffffu, incl, 31);
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            int idx = lane * PER + q;
+            s_off[idx / (kET / 32)][idx % (kET / 32)] = run;
+            run += c[q];
+        }
+        int64_t pre = lookback(status, tile, tot, 0, err);
+        if (lane == 0) {
+            s_prefix = pre;
+            const int64_t ntiles = (n_in + kETile - 1) / kETile;
+            if (tile == ntiles - 1) *d_count = pre + tot;
+        }
+    }
+    __syncthreads();
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int it = 0; it < kEI; ++it) {
+        if (bal[it] & (1u << lane)) {
+            int64_t pos = s_prefix + s_off[it][warp] + __popc(bal[it] & lt);
+            eout[pos] = k[it];
+        }
+    }
+}
+
+// rowid[e] = v for every entry e of row v (entries outside every row stay -1)
+__global__ void k_rowid(const int32_t *first, const int32_t *deg, int32_t V, int64_t E,
+                        int32_t *rowid, int *err)
+{
+    const int lane = threadIdx.x & 31;
+    for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V;
+         v += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        int64_t f = first[v], d = deg[v];
+        if (f < 0 || d < 0 || f + d > E) {
+            if (lane == 0) set_err(err, DEV_BAD_INPUT);
+            continue;
+        }
+        for (int64_t e = f + lane; e < f + d; e += 32) rowid[e] = (int32_t)v;
+    }
+}
+
+// Both directions of every entry of an upper-triangle CSR with uint8 weights.
+// Forward copies land at [e], reverse copies at [nnz + e].
+template <int MODE>
+__global__ void k_edges_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w,
+                              int32_t n, int64_t nnz, Pack pk, uint64_t *eout,
+                              unsigned long long *best, int *err)
+{
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
+         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int64_t s = indptr[i], e_end = indptr[i + 1];
+        if (s < 0 || e_end < s || e_end > nnz) {
+            if (lane == 0) set_err(err, DEV_BAD_INPUT);
+            continue;
+        }
+        uint64_t m = kNone;
+        for (int64_t e = s + lane; e < e_end; e += 32) {
+            int32_t j = indices[e];
+            if (j <= i || j >= n) {
+                set_err(err, DEV_BAD_INPUT);
+                eout[e] = kNone;       // never selected: dropped by the first contraction
+                eout[nnz + e] = kNone;
+                continue;
+            }
+            uint32_t ww = w[e];
+            uint64_t f = pk.make(ww, (uint32_t)i, (uint32_t)j);
+            eout[e] = f;
+            eout[nnz + e] = f | 1ull;
+            uint64_t sel_f = MODE == SEL_MST ? (f >> 1) : (((uint64_t)ww << 32) | (uint32_t)j);
+            uint64_t sel_r = MODE == SEL_MST ? (f >> 1) : (((uint64_t)ww << 32) | (uint32_t)i);
+            m = sel_f < m ? sel_f : m;
+            atomicMin(&best[j], (unsigned long long)sel_r);
+        }
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {
+            uint64_t o = __shfl_xor_sync(0xffffffffu, m, d);
+            m = o < m ? o : m;
+        }
+        if (lane == 0 && m != kNone) atomicMin(&best[i], (unsigned long long)m);
+    }
+}
+
+__global__ void k_iota(int32_t *a, int64_t n)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        a[i] = (int32_t)i;
+}
+
+// successor of each supervertex from its selected key
+template <int MODE>
+__global__ void k_select(const unsigned long long *best, int32_t *succ, int32_t V,
+                         const int32_t *label, Pack pk)
+{
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t b = best[s];
+        int32_t t = (int32_t)s;
+        if (b != kNone) {
+            if (MODE == SEL_CC) {
+                t = (int32_t)(uint32_t)b;
+            } else {
+                int32_t la = label[pk.sel_a(b)], lb = label[pk.sel_b(b)];
+                t = (la == (int32_t)s) ? lb : la;
+            }
+        }
+        succ[s] = t;
+    }
+}
+
+// mutual picks: the smaller id drops its edge (MyML/MyML/graph/mst.py:283-305)
+__global__ void k_mirror(const int32_t *succ, int32_t *color, int32_t *emit, int32_t V)
+{
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        int32_t t = succ[s];
+        bool has = t != (int32_t)s;
+        bool drop = has && succ[t] == (int32_t)s && (int32_t)s < t;
+        color[s] = (has && !drop) ? t : (int32_t)s;
+        if (emit) emit[s] = (has && !drop) ? 1 : 0;
+    }
+}
+
+__global__ void k_emit(const unsigned long long *best, const int32_t *emit, const int32_t *pos,
+                       uint64_t *out, int32_t V)
+{
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
+         s += (int64_t)gridDim.x * blockDim.x)
+        if (emit[s]) out[pos[s]] = best[s];
+}
+
+// roots by pointer chasing with path halving; bounded (a non-forest errors)
+__global__ void k_jump(int32_t *color, int32_t V, int *err)
+{
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        int32_t c = color[s];
+        int64_t guard = 0;
+        while (true) {
+            int32_t p = color[c];
+            if (p == c) break;
+            int32_t g = color[p];
+            if (g != p) color[c] = g;      // halving: benign race, stays an ancestor
+            c = g;
+            if (++guard > (int64_t)V + 64) {
+                set_err(err, DEV_CHASE_LIMIT);
+                break;
+            }
+        }
+        color[s] = c;
+    }
+}
+
+__global__ void k_rootflag(const int32_t *color, int32_t *flag, int32_t V)
+{
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
+         s += (int64_t)gridDim.x * blockDim.x)
+        flag[s] = color[s] == (int32_t)s;
+}
+
+__global__ void k_relabel(int32_t *label, const int32_t *color, const int32_t *newid, int64_t V0)
+{
+    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < V0;
+         x += (int64_t)gridDim.x * blockDim.x)
+        label[x] = newid[color[label[x]]];
+}
+
+// MST selection key -> index of its entry in row min(u,v) of a symmetric CSR
+template <typename WT>
+__global__ void k_key2eid(const uint64_t *keys, int64_t n_keys, const int32_t *first,
+                          const int32_t *deg, const int32_t *dest, const WT *weight, Pack pk,
+                          int32_t *out, int *err)
+{
+    const int lane = threadIdx.x & 31;
+    for (int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n_keys;
+         q += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        uint64_t s = keys[q];
+        int32_t a = (int32_t)pk.sel_a(s), b = (int32_t)pk.sel_b(s);
+        uint32_t w = pk.sel_w(s);
+        int64_t f = first[a], d = deg[a];
+        int64_t found = -1;
+        for (int64_t e0 = f; e0 < f + d && found < 0; e0 += 32) {
+            int64_t e = e0 + lane;
+            bool hit = e < f + d && dest[e] == b && wword(weight[e]) == w;
+            unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (m) found = e0 + __ffs(m) - 1;
+        }
+        if (lane == 0) {
+            if (found < 0) set_err(err, DEV_BAD_INPUT);   // graph not symmetric
+            out[q] = (int32_t)found;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side engine
+// ---------------------------------------------------------------------------
+struct Engine {
+    int *err;
+    int64_t *cnt;             // [0] edges out, [1] vertices out, [2] emitted
+    uint64_t *ea, *eb;
+    int32_t *label;
+    unsigned long long *best;
+    int32_t *succ, *color, *flag, *pos;
+    uint64_t *mst;
+    ScanScratch scan;
+    int32_t V0;
+    int64_t Emax;
+
+    static Engine carve(Carver &c, int32_t V0, int64_t Emax)
+    {
+        Engine g;
+        g.err = c.take<int>(1);
+        g.cnt = c.take<int64_t>(4);
+        g.V0 = V0;
+        g.Emax = Emax;
+        g.ea = c.take<uint64_t>(Emax > 0 ? Emax : 1);
+        g.eb = c.take<uint64_t>(Emax > 0 ? Emax : 1);
+        g.label = c.take<int32_t>(V0);
+        g.best = c.take<unsigned long long>(V0);
+        g.succ = c.take<int32_t>(V0);
+        g.color = c.take<int32_t>(V0);
+        g.flag = c.take<int32_t>(V0);
+        g.pos = c.take<int32_t>(V0);
+        g.mst = c.take<uint64_t>(V0);
+        g.scan = ScanScratch::carve(c, Emax > V0 ? Emax : V0, g.err);
+        return g;
+    }
+
+    int read_counts(cudaStream_t st, int64_t h[3])
+    {
+        int e = 0;
+        EACB_CUDA(cudaMemcpyAsync(h, cnt, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        EACB_CUDA(cudaStreamSynchronize(st));
+        return dev_err_to_status(e);
+    }
+
+    int reset(cudaStream_t st)
+    {
+        EACB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+        EACB_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int64_t), st));
+        EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V0, st));
+        k_iota<<<grid_for(V0, 256), 256, 0, st>>>(label, V0);
+        EACB_CHECK_LAUNCH();
+        return EACB_OK;
+    }
+
+    template <int MODE, typename Src>
+    int filter(const Src &src, int64_t n_in, uint64_t *out, cudaStream_t st)
+    {
+        if (n_in == 0) {
+            EACB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int64_t), st));
+            return EACB_OK;
+        }
+        const int64_t ntiles = (n_in + kETile - 1) / kETile;
+        EACB_CUDA(cudaMemsetAsync(scan.status, 0, sizeof(uint64_t) * ntiles, st));
+        EACB_CUDA(cudaMemsetAsync(scan.counter, 0, sizeof(int), st));
+        k_edge_tile<MODE, Src><<<(unsigned)ntiles, kET, 0, st>>>(
+            src, n_in, out, best, scan.status, scan.counter, cnt, err);
+        EACB_CHECK_LAUNCH();
+        return EACB_OK;
+    }
+
+    // Rounds; edges of round 0 are in `ea` (E0 of them) and `best` holds
+    // their selection.  On return: label = component of every vertex,
+    // *n_comp = number of components, *n_mst = emitted forest edges.
+    template <int MODE>
+    int run(Pack pk, int64_t E0, cudaStream_t st, int64_t *n_mst_out, int64_t *n_comp_out)
+    {
+        int32_t V = V0;
+        int64_t E = E0;
+        int64_t n_mst = 0;
+        uint64_t *ein = ea, *eout = eb;
+        for (int round = 0; round < 96; ++round) {
+            const unsigned gv = grid_for(V, 256);
+            k_select<MODE><<<gv, 256, 0, st>>>(best, succ, V, label, pk);
+            EACB_CHECK_LAUNCH();
+            k_mirror<<<gv, 256, 0, st>>>(succ, color, MODE == SEL_MST ? flag : nullptr, V);
+            EACB_CHECK_LAUNCH();
+            if (MODE == SEL_MST) {
+                int s = scan_launch<int32_t, int32_t>(flag, pos, V, 0, &cnt[2], scan, st);
+                if (s) return s;
+                k_emit<<<gv, 256, 0, st>>>(best, flag, pos, mst + n_mst, V);
+                EACB_CHECK_LAUNCH();
+            }
+            k_jump<<<gv, 256, 0, st>>>(color, V, err);
+            EACB_CHECK_LAUNCH();
+            k_rootflag<<<gv, 256, 0, st>>>(color, flag, V);
+            EACB_CHECK_LAUNCH();
+            int s = scan_launch<int32_t, int32_t>(flag, pos, V, 0, &cnt[1], scan, st);
+            if (s) return s;
+            k_relabel<<<grid_for(V0, 256), 256, 0, st>>>(label, color, pos, V0);
+            EACB_CHECK_LAUNCH();
+            EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V, st));
+            SrcEdges se{ein, label, pk, (uint32_t)V0};
+            cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+            const bool timed = prof().enabled != 0;
+            if (timed) {
+                cudaEventCreate(&ev0);
+                cudaEventCreate(&ev1);
+                cudaEventRecord(ev0, st);
+            }
+            s = filter<MODE>(se, E, eout, st);
+            if (s) return s;
+            if (timed) cudaEventRecord(ev1, st);
+            int64_t h[3];
+            s = read_counts(st, h);
+            if (s) return s;
+            if (timed) {
+                // algorithmic HBM bytes of one contraction: every edge word read
+                // once, every surviving edge word written once
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev0, ev1);
+                prof().ms[PROF_EDGE_TILE] += ms;
+                prof().bytes[PROF_EDGE_TILE] += 8.0 * (double)E + 8.0 * (double)h[0];
+                prof().count[PROF_EDGE_TILE] += 1;
+                cudaEventDestroy(ev0);
+                cudaEventDestroy(ev1);
+            }
+            if (MODE == SEL_MST) n_mst += h[2];
+            int32_t Vn = (int32_t)h[1];
+            int64_t En = h[0];
+            uint64_t *t = ein;
+            ein = eout;
+            eout = t;
+            if (Vn <= 1 || En == 0) {
+                *n_mst_out = n_mst;
+                *n_comp_out = Vn;
+                return EACB_OK;
+            }
+            if (Vn >= V) return EACB_ERR_NOT_CONVERGED;
+            V = Vn;
+            E = En;
+        }
+        return EACB_ERR_NOT_CONVERGED;
+    }
+};
+
+template <typename WT>
+static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wbits,
+                         const int32_t *first, const int32_t *deg, int32_t V, int64_t E,
+                         int32_t *mst_out, int64_t *host_n_mst, int32_t *labels_out,
+                         int64_t *host_n_comp, void *ws, size_t ws_bytes, cudaStream_t st)
+{
+    Pack pk;
+    int s = make_pack(V, wbits, pk);
+    if (s) return s;
+    Carver c(ws, ws_bytes);
+    Engine g = Engine::carve(c, V, E);
+    int32_t *rowid = c.take<int32_t>(E > 0 ? E : 1);
+    if (c.overflow) return EACB_ERR_WORKSPACE;
+    if ((s = g.reset(st))) return s;
+    if (E > 0) {
+        EACB_CUDA(cudaMemsetAsync(rowid, 0xff, sizeof(int32_t) * E, st));
+        k_rowid<<<grid_for((int64_t)V * 32, 256), 256, 0, st>>>(first, deg, V, E, rowid, g.err);
+        EACB_CHECK_LAUNCH();
+    }
+    SrcCSR<WT> src{rowid, dest, weight, V, pk, g.err};
+    int64_t h[3];
+    if (mode == SEL_MST) s = g.filter<SEL_MST>(src, E, g.ea, st);
+    else s = g.filter<SEL_CC>(src, E, g.ea, st);
+    if (s) return s;
+    if ((s = g.read_counts(st, h))) return s;
+    int64_t n_mst = 0, n_comp = 0;
+    if (mode == SEL_MST) s = g.run<SEL_MST>(pk, h[0], st, &n_mst, &n_comp);
+    else s = g.run<SEL_CC>(pk, h[0], st, &n_mst, &n_comp);
+    if (s) return s;
+    if (mode == SEL_MST) {
+        if (n_mst > 0) {
+            k_key2eid<WT><<<grid_for(n_mst * 32, 256), 256, 0, st>>>(g.mst, n_mst, first, deg, dest,
+                                                                      weight, pk, mst_out, g.err);
+            EACB_CHECK_LAUNCH();
+        }
+        if ((s = g.read_counts(st, h))) return s;
+        *host_n_mst = n_mst;
+    } else {
+        EACB_CUDA(cudaMemcpyAsync(labels_out, g.label, sizeof(int32_t) * V,
+                                  cudaMemcpyDeviceToDevice, st));
+        *host_n_comp = n_comp;
+    }
+    return EACB_OK;
+}
+
+static int csr_dispatch(int mode, const int32_t *dest, const void *weight, int dt,
+                        const int32_t *first, const int32_t *deg, int32_t V, int64_t E,
+                        int32_t *mst_out, int64_t *host_n_mst, int32_t *labels,
+                        int64_t *host_n_comp, void *ws, size_t ws_bytes, uintptr_t stream)
+{
+    if (V <= 0 || E < 0 || !first || !deg || (E > 0 && (!dest || !weight)) || !ws)
+        return EACB_ERR_BAD_ARGUMENT;
+    cudaStream_t st = as_stream(stream);
+    const int wb = dtype_bits(dt);
+    switch (dt) {
+    case EACB_U8:
+        return csr_graph_run<uint8_t>(mode, dest, (const uint8_t *)weight, wb, first, deg, V, E,
+                                      mst_out, host_n_mst, labels, host_n_comp, ws, ws_bytes, st);
+    case EACB_U16:
+        return csr_graph_run<uint16_t>(mode, dest, (const uint16_t *)weight, wb, first, deg, V, E,
+                                       mst_out, host_n_mst, labels, host_n_comp, ws, ws_bytes, st);
+    case EACB_I32:
+        return csr_graph_run<int32_t>(mode, dest, (const int32_t *)weight, wb, first, deg, V, E,
+                                      mst_out, host_n_mst, labels, host_n_comp, ws, ws_bytes, st);
+    case EACB_U32:
+        return csr_graph_run<uint32_t>(mode, dest, (const uint32_t *)weight, wb, first, deg, V, E,
+                                       mst_out, host_n_mst, labels, host_n_comp, ws, ws_bytes, st);
+    case EACB_F32:
+        return csr_graph_run<float>(mode, dest, (const float *)weight, wb, first, deg, V, E,
+                                    mst_out, host_n_mst, labels, host_n_comp, ws, ws_bytes, st);
+    default:
+        return EACB_ERR_BAD_ARGUMENT;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Final clustering helpers
+// ---------------------------------------------------------------------------
+__global__ void k_weight_hist(const uint64_t *keys, int64_t n, Pack pk, int64_t *hist)
+{
+    __shared__ int64_t h[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd((unsigned long long *)&h[pk.sel_w(keys[i]) & 255], 1ull);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        if (h[i]) atomicAdd((unsigned long long *)&hist[i], (unsigned long long)h[i]);
+}
+
+struct CutPlan {
+    int64_t status;      // 0 ok, else an eacb status
+    int64_t n_clusters;  // nc_stable
+    int64_t wmax;        // keep forest edges with weight <= wmax (-1: none)
+    int64_t need_labels;
+};
+
+// The lifetime rule of MyML/MyML/EAC/eac.py:366-391 and the cut decision of
+// :220-265, evaluated on the 256-bin histogram of the uint8 MST weights
+// (sorted weights are the bins expanded in order).
+__global__ void k_cut_plan(const int64_t *hist, int64_t n_mst, int32_t n, int32_t max_dist,
+                           int32_t n_clusters, CutPlan *plan)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    CutPlan p{0, 0, 255, 0};
+    const int64_t n_disc = (int64_t)n - n_mst;
+    int64_t nc;
+    int64_t thr = 255;
+    if (n_clusters == 0) {
+        if (n_mst < 2) { p.status = EACB_ERR_VALUE; *plan = p; return; }
+        // lifetimes = differences of consecutive sorted weights; zero ones
+        // exist iff some bin holds two or more edges
+        bool has_zero = false;
+        int prev = -1, wlast = 0;
+        int best_gap = 0, m_w = -1;
+        for (int b = 0; b < 256; ++b) {
+            int64_t c = hist[b];
+            if (!c) continue;
+            if (c >= 2) has_zero = true;
+            if (prev >= 0 && b - prev > best_gap) { best_gap = b - prev; m_w = prev; }
+            prev = b;
+            wlast = b;
+        }
+        if (!has_zero) { p.status = EACB_ERR_VALUE; *plan = p; return; }
+        int first_w = -1;
+        for (int b = 0; b < 256; ++b) if (hist[b]) { first_w = b; break; }
+        if (m_w < 0) m_w = first_w;          // all lifetimes zero: argmax = 0
+        int64_t above = 0;
+        for (int b = m_w + 1; b < 256; ++b) above += hist[b];
+        int64_t cont = above == 0 ? 1 : above + 1;
+        // th < 2 * min(zero lifetimes) never holds once a zero lifetime exists
+        if (n_disc > 1) {
+            int64_t disc_life = (int64_t)max_dist + 1 + 1 - wlast;
+            if ((int64_t)best_gap > disc_life) cont += n_disc - 1;
+            else cont = n_disc;
+        }
+        nc = cont;
+        thr = m_w;    // the cut removes exactly the edges heavier than w[m]
+    } else {
+        nc = n_clusters;
+        if (nc > n_disc) {
+            // cut the (nc - n_disc) heaviest forest edges; supported when that
+            // boundary falls between two weight bins (no tie to split)
+            const int64_t n_cuts = nc - n_disc;
+            int64_t acc = 0;
+            thr = 255;
+            for (int b = 255; b >= 0 && acc < n_cuts; --b) {
+                if (acc + hist[b] > n_cuts) { p.status = EACB_ERR_UNSUPPORTED; *plan = p; return; }
+                acc += hist[b];
+                thr = b - 1;
+            }
+        }
+    }
+    p.n_clusters = nc;
+    p.wmax = (nc > n_disc) ? thr : 255;
+    p.need_labels = nc > 1;
+    *plan = p;
+}
+
+__global__ void k_comp_min(const int32_t *label, int32_t n, int32_t *cmin)
+{
+    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n;
+         x += (int64_t)gridDim.x * blockDim.x)
+        atomicMin(&cmin[label[x]], (int32_t)x);
+}
+
+__global__ void k_first_flag(const int32_t *label, const int32_t *cmin, int32_t n, int32_t *flag)
+{
+    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n;
+         x += (int64_t)gridDim.x * blockDim.x)
+        flag[x] = cmin[label[x]] == (int32_t)x;
+}
+
+__global__ void k_canon(const int32_t *label, const int32_t *cmin, const int32_t *pos, int32_t n,
+                        int32_t *out)
+{
+    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n;
+         x += (int64_t)gridDim.x * blockDim.x)
+        out[x] = pos[cmin[label[x]]];
+}
+
+}  // namespace eacb
+
+using namespace eacb;
+
+extern "C" size_t eacb_boruvka_workspace_size(int32_t n_vertices, int64_t n_edges)
+{
+    Carver c(nullptr, 0);
+    Engine::carve(c, n_vertices, n_edges);
+    c.take<int32_t>(n_edges > 0 ? n_edges : 1);
+    return c.off;
+}
+
+extern "C" int eacb_boruvka_mst(const int32_t *dest, const void *weight, int weight_dtype,
+                                const int32_t *first_edge, const int32_t *out_degree,
+                                int32_t n_vertices, int64_t n_edges, int32_t *mst_out,
+                                int64_t *host_n_mst, void *ws, size_t ws_bytes, uintptr_t stream)
+{
+    if (!host_n_mst || (!mst_out && n_vertices > 1)) return EACB_ERR_BAD_ARGUMENT;
+    int64_t dummy = 0;
+    return csr_dispatch(SEL_MST, dest, weight, weight_dtype, first_edge, out_degree, n_vertices,
+                        n_edges, mst_out, host_n_mst, nullptr, &dummy, ws, ws_bytes, stream);
+}
+
+extern "C" int eacb_connected_components(const int32_t *dest, const void *weight,
+                                         int weight_dtype, const int32_t *first_edge,
+                                         const int32_t *out_degree, int32_t n_vertices,
+                                         int64_t n_edges, int32_t *labels, int64_t *host_n_comps,
+                                         void *ws, size_t ws_bytes, uintptr_t stream)
+{
+    if (!labels || !host_n_comps) return EACB_ERR_BAD_ARGUMENT;
+    int64_t dummy = 0;
+    return csr_dispatch(SEL_CC, dest, weight, weight_dtype, first_edge, out_degree, n_vertices,
+                        n_edges, nullptr, &dummy, labels, host_n_comps, ws, ws_bytes, stream);
+}
+
+static void carve_final(Carver &c, int32_t n, int64_t nnz, Engine *g, int64_t **hist,
+                        CutPlan **plan, int32_t **cmin)
+{
+    int64_t emax = 2 * nnz > 2 * (int64_t)n ? 2 * nnz : 2 * (int64_t)n;
+    *g = Engine::carve(c, n, emax);
+    *hist = c.take<int64_t>(256);
+    *plan = c.take<CutPlan>(1);
+    *cmin = c.take<int32_t>(n);
+}
+
+extern "C" size_t eacb_final_clustering_workspace_size(int32_t n, int64_t nnz)
+{
+    Carver c(nullptr, 0);
+    Engine g;
+    int64_t *h;
+    CutPlan *p;
+    int32_t *m;
+    carve_final(c, n, nnz, &g, &h, &p, &m);
+    return c.off;
+}
+
+extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indices,
+                                     const uint8_t *diassoc, int32_t n, int64_t nnz,
+                                     int32_t max_dist, int32_t n_clusters, int32_t *labels,
+                                     int64_t *host_n_fclusts, int32_t *host_labels_valid,
+                                     void *ws, size_t ws_bytes, uintptr_t stream)
+{
+    if (n <= 0 || nnz < 0 || !indptr || (nnz > 0 && (!indices || !diassoc)) || !labels ||
+        !host_n_fclusts || !host_labels_valid || !ws || n_clusters < 0)
+        return EACB_ERR_BAD_ARGUMENT;
+    cudaStream_t st = as_stream(stream);
+    Pack pk;
+    int s = make_pack(n, 8, pk);
+    if (s) return s;
+    Carver c(ws, ws_bytes);
+    Engine g;
+    int64_t *hist;
+    CutPlan *plan;
+    int32_t *cmin;
+    carve_final(c, n, nnz, &g, &hist, &plan, &cmin);
+    if (c.overflow) return EACB_ERR_WORKSPACE;
+    if ((s = g.reset(st))) return s;
+    // 1. minimum spanning forest of the dissimilarity graph
+    if (nnz > 0) {
+        k_edges_upper<SEL_MST><<<grid_for((int64_t)n * 32, 256), 256, 0, st>>>(
+            indptr, indices, diassoc, n, nnz, pk, g.ea, g.best, g.err);
+        EACB_CHECK_LAUNCH();
+    }
+    int64_t h0[3];
+    if ((s = g.read_counts(st, h0))) return s;     // input validity before the rounds
+    int64_t n_mst = 0, n_comp = 0;
+    if ((s = g.run<SEL_MST>(pk, 2 * nnz, st, &n_mst, &n_comp))) return s;
+    // 2. lifetime rule on the weight histogram
+    EACB_CUDA(cudaMemsetAsync(hist, 0, 256 * sizeof(int64_t), st));
+    if (n_mst > 0) {
+        k_weight_hist<<<grid_for(n_mst, 256, 148 * 4), 256, 0, st>>>(g.mst, n_mst, pk, hist);
+        EACB_CHECK_LAUNCH();
+    }
+    k_cut_plan<<<1, 32, 0, st>>>(hist, n_mst, n, max_dist, n_clusters, plan);
+    EACB_CHECK_LAUNCH();
+    CutPlan hp;
+    EACB_CUDA(cudaMemcpyAsync(&hp, plan, sizeof(CutPlan), cudaMemcpyDeviceToHost, st));
+    EACB_CUDA(cudaStreamSynchronize(st));
+    if (hp.status) return (int)hp.status;
+    *host_n_fclusts = hp.n_clusters;
+    if (!hp.need_labels) {
+        *host_labels_valid = 0;
+        *host_n_fclusts = 1;
+        return EACB_OK;
+    }
+    // 3. components of the forest without the cut edges (the forest keys
+    //    move to ea: the second run reuses the engine's buffers)
+    EACB_CUDA(cudaMemcpyAsync(g.ea, g.mst, sizeof(uint64_t) * n_mst, cudaMemcpyDeviceToDevice, st));
+    if ((s = g.reset(st))) return s;
+    // the forest edges (both directions) go from ea[0, n_mst) into eb
+    SrcForest sf{g.ea, n_mst, hp.wmax, pk};
+    if ((s = g.filter<SEL_CC>(sf, 2 * n_mst, g.eb, st))) return s;
+    int64_t h[3];
+    if ((s = g.read_counts(st, h))) return s;
+    // run() starts from ea: swap roles by copying (forest is small)
+    EACB_CUDA(cudaMemcpyAsync(g.ea, g.eb, sizeof(uint64_t) * h[0], cudaMemcpyDeviceToDevice, st));
+    int64_t nm2 = 0, nc2 = 0;
+    if ((s = g.run<SEL_CC>(pk, h[0], st, &nm2, &nc2))) return s;
+    // 4. number components by their smallest member
+    EACB_CUDA(cudaMemsetAsync(cmin, 0x7f, sizeof(int32_t) * n, st));
+    const unsigned gn = grid_for(n, 256);
+    k_comp_min<<<gn, 256, 0, st>>>(g.label, n, cmin);
+    EACB_CHECK_LAUNCH();
+    k_first_flag<<<gn, 256, 0, st>>>(g.label, cmin, n, g.flag);
+    EACB_CHECK_LAUNCH();
+    if ((s = scan_launch<int32_t, int32_t>(g.flag, g.pos, n, 0, &g.cnt[1], g.scan, st))) return s;
+    k_canon<<<gn, 256, 0, st>>>(g.label, cmin, g.pos, n, labels);
+    EACB_CHECK_LAUNCH();
+    if ((s = g.read_counts(st, h))) return s;
+    *host_n_fclusts = h[1];
+    *host_labels_valid = 1;
+    return EACB_OK;
+}

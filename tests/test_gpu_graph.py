@@ -1,0 +1,169 @@
+"""GPU parity: scan, Boruvka MST, connected components and the EAC final
+clustering against the oracle and the reference's golden outputs."""
+import numpy as np
+import pytest
+
+import oracle
+from tests.conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def T():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def test_scan_golden(T):
+    from masters_final_b200.utils.scan import exprefixsumNumba, scan_gpu, exprefixsumNumbaSingle
+    g = golden("scan")
+    out = np.empty_like(g["small_in"])
+    assert exprefixsumNumba(g["small_in"], out) == g["small_total"]
+    assert np.array_equal(out, g["small_out"])
+    out = np.empty_like(g["wrap_in"])
+    assert exprefixsumNumba(g["wrap_in"], out) == g["wrap_total"]
+    assert np.array_equal(out, g["wrap_out"])
+    a64 = g["wrap_in"].astype(np.int64)
+    out = np.empty_like(a64)
+    assert exprefixsumNumba(a64, out) == g["i64_total"]
+    assert np.array_equal(out, g["i64_out"])
+    d = g["single_in"].copy()
+    assert exprefixsumNumbaSingle(d, 7) == g["single_total"]
+    assert np.array_equal(d, g["single_out"])
+    x = g["small_in"].copy()
+    assert scan_gpu(x) == g["small_total"]
+    assert np.array_equal(x, g["small_out"])
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 31, 4095, 4096, 4097, 2048 * 3 + 5, 1 << 20, 3_000_001])
+def test_scan_sizes(T, n):
+    from masters_final_b200.utils.scan import exprefixsumNumba
+    rng = np.random.default_rng(n)
+    a = rng.integers(-1000, 100000, n).astype(np.int32)
+    out = np.empty_like(a)
+    tot = exprefixsumNumba(a, out, init=3)
+    ref, rt = oracle.exprefixsum(a, init=3)
+    assert tot == rt
+    assert np.array_equal(out, ref)
+
+
+def test_scan_64m_device_property(T):
+    """The full-size stream (64 Mi int32 uniform in [0, 1000]) on device:
+    differences of the output give back the input, and the total is exact."""
+    from masters_final_b200 import workloads as W
+    from masters_final_b200.utils.scan import scan_gpu
+    a = W.scan_input(64 << 20, seed=3)
+    d = T.from_numpy(a).cuda()
+    x = d.clone()
+    tot = scan_gpu(x)
+    assert int(tot.item()) == int(a.astype(np.int64).sum())
+    assert T.equal((x[1:] - x[:-1]), d[:-1])
+    assert int(x[0].item()) == 0
+
+
+def _check_mst(indptr, dest, w, mst, n):
+    V = indptr.size - 1
+    rows = np.repeat(np.arange(V), np.diff(indptr))
+    a, b = rows[mst[:n]], dest[mst[:n]]
+    assert np.all(a < b)
+    ua, ub, uw = oracle.upper_edges(indptr, dest, w)
+    f = oracle.kruskal_forest(V, ua, ub, uw)
+    got = set(zip(a.tolist(), b.tolist()))
+    exp = set(zip(ua[f].tolist(), ub[f].tolist()))
+    assert got == exp
+    return w[mst[:n]].astype(np.int64).sum()
+
+
+@pytest.mark.parametrize("name", ["graph_4elt", "graph_knn20k", "graph_disconnected"])
+def test_boruvka_golden(T, name):
+    from masters_final_b200.graph.mst import boruvka_minho_gpu
+    g = golden(name)
+    indptr, dest, w = g["indptr"], g["indices"], g["data"]
+    first = indptr[:-1].astype(np.int32)
+    deg = np.diff(indptr).astype(np.int32)
+    mst, n = boruvka_minho_gpu(dest, w, first, deg)
+    assert n == g["n_mst"]
+    assert _check_mst(indptr, dest, w, mst, n) == g["mst_weight"]
+
+
+@pytest.mark.parametrize("name", ["graph_4elt", "graph_knn20k", "graph_disconnected"])
+def test_connected_components_golden(T, name):
+    from masters_final_b200.graph.connected_components import connected_comps_gpu
+    g = golden(name)
+    indptr, dest, w = g["indptr"], g["indices"], g["data"]
+    labels = connected_comps_gpu(dest, w, indptr[:-1].astype(np.int32),
+                                 np.diff(indptr).astype(np.int32))
+    assert np.array_equal(labels, g["cc_labels"])
+
+
+def test_boruvka_knn_1m_properties(T):
+    """The full-size graph (1M points, 16-NN, uint8 weights): the forest is
+    exactly the oracle Kruskal forest under (w, min, max)."""
+    from masters_final_b200 import workloads as W
+    from masters_final_b200.graph.mst import boruvka_minho_gpu
+    indptr, dest, w = W.knn_graph(1_000_000, k=16, seed=2)
+    mst, n = boruvka_minho_gpu(dest, w, indptr[:-1].astype(np.int32),
+                               np.diff(indptr).astype(np.int32))
+    assert n == 999_999
+    _check_mst(indptr, dest, w, mst, n)
+
+
+@pytest.mark.parametrize("dt", [np.uint16, np.int32, np.float32])
+def test_boruvka_weight_types(T, dt):
+    from masters_final_b200 import workloads as W
+    from masters_final_b200.graph.mst import boruvka_minho_gpu
+    rng = np.random.default_rng(7)
+    indptr, dest, w8 = W.knn_graph(3000, k=8, seed=5)
+    ua, ub, _ = oracle.upper_edges(indptr, dest, w8)
+    if dt == np.float32:
+        uw = rng.standard_normal(ua.size).astype(np.float32)
+    else:
+        uw = rng.integers(0 if dt == np.uint16 else -50, 50, ua.size).astype(dt)
+    ip, d, w = W.csr_from_undirected(3000, ua, ub, uw)
+    mst, n = boruvka_minho_gpu(d, w, ip[:-1].astype(np.int32), np.diff(ip).astype(np.int32))
+    f = oracle.kruskal_forest(3000, ua, ub, uw)
+    assert n == f.sum()
+    _check_mst(ip, d, w, mst, n)
+
+
+def test_final_clustering_golden(T):
+    from masters_final_b200.EAC.eac import sp_sl_lifetime_csr
+    for name in ("eac_small", "eac_discard"):
+        g = golden(name)
+        n = g["x"].shape[0]
+        nc, labels = sp_sl_lifetime_csr(g["indptr"], g["indices"], g["diassoc"], n, int(g["P"]))
+        assert nc == g["n_fclusts"]
+        assert np.array_equal(labels, g["final_labels"])
+
+
+def test_final_clustering_disconnected(T):
+    """Isolated points and separate groups exercise the disconnected-graph
+    branch of the lifetime rule (MyML/MyML/EAC/eac.py:238-248)."""
+    from masters_final_b200.EAC.eac import sp_sl_lifetime_csr
+    rng = np.random.default_rng(3)
+    n = 5000
+    groups = rng.integers(0, 7, n)
+    groups[:50] = -1                      # isolated
+    a, b = [], []
+    for gidx in range(7):
+        m = np.nonzero(groups == gidx)[0]
+        for _ in range(6):
+            x, y = rng.choice(m, 2 * m.size).reshape(2, -1)
+            keep = x != y
+            a.append(np.minimum(x, y)[keep])
+            b.append(np.maximum(x, y)[keep])
+    a, b = np.concatenate(a), np.concatenate(b)
+    key = np.unique(a * n + b)
+    a, b = key // n, key % n
+    w = rng.integers(1, 30, a.size).astype(np.uint8)
+    order = np.lexsort((b, a))
+    a, b, w = a[order], b[order], w[order]
+    indptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(a, minlength=n), out=indptr[1:])
+    for P in (29, 40):
+        nc, labels = sp_sl_lifetime_csr(indptr, b.astype(np.int32), w, n, P)
+        nc2, lab2 = oracle.sp_sl_lifetime(n, a, b, w, P)
+        assert nc == nc2
+        assert np.array_equal(labels, lab2)
