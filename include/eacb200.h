@@ -122,6 +122,91 @@ int eacb_connected_components(const int32_t *dest, const void *weight, int weigh
                               void *ws, size_t ws_bytes, uintptr_t stream);
 
 /* ------------------------------------------------------------------------
+ * K-Means ensemble (batched Lloyd iterations, all partitions at once).
+ * Replaces MyML/MyML/utils/partition.py:88-124 (generateEnsemble) running
+ * MyML/MyML/cluster/KMeans.py:117-189 (K_Means.fit) per partition, with the
+ * label step :453-490 / :586-629 and the centroid step :709-754
+ * (empty clusters take the points of MyML/MyML/utils/sorting.py:9-47).
+ * X: n x d float32 row-major (d <= 32).  Partition p has k[p] <= kmax
+ * clusters (device int32[P]) and starts from the points init[p*kmax + c],
+ * c < k[p] (device int32; the host draws them like the reference, with
+ * random.sample).  Each partition runs until max_iter label passes or until
+ * its inertia (numpy float32 sum of the distances) changes by at most tol.
+ * label_mode 0 = float32 screen + exact re-check (CUDA cores),
+ *            1 = tcgen05 tensor cores + exact re-check;
+ * both return the reference's labels exactly.  centroid_mode 0 = float32
+ * sums in point order (the reference's arithmetic), 1 = float64 sums.
+ * Outputs: labels (P*n int32), centroids (P*kmax*d float32, rows c < k[p]),
+ * optional dists (P*n float32), iters (P int32), inertia (P float32).
+ * ------------------------------------------------------------------------ */
+size_t eacb_kmeans_workspace_size(int32_t n, int32_t d, int32_t P, int32_t kmax);
+int eacb_kmeans_ensemble(const float *X, int32_t n, int32_t d, int32_t P,
+                         const int32_t *k, int32_t kmax, const int32_t *init,
+                         int32_t max_iter, float tol, int32_t label_mode,
+                         int32_t centroid_mode, int32_t *labels, float *centroids,
+                         float *dists, int32_t *iters, float *inertia,
+                         void *ws, size_t ws_bytes, uintptr_t stream);
+
+/* One label step for given centroids (k x d float32): the reference's
+ * labels and float32 distances (KMeans.py:453-490). */
+size_t eacb_kmeans_label_workspace_size(int32_t n, int32_t d, int32_t k);
+int eacb_kmeans_label(const float *X, int32_t n, int32_t d, const float *C, int32_t k,
+                      int32_t label_mode, int32_t *labels, float *dists,
+                      void *ws, size_t ws_bytes, uintptr_t stream);
+
+/* ------------------------------------------------------------------------
+ * Sparse co-association matrix, condensed (row i holds columns j > i).
+ * Replaces MyML/MyML/EAC/sparse.py:154-226 (EAC_CSR.update_ensemble with
+ * update_cluster_fp_condensed :446-465 and
+ * update_cluster_sorted_surgical_condensed :957-1040, then _condense).
+ * The ensemble is a label matrix labels[p*n + i] (cluster id in [0, K) of
+ * point i in partition p, -1 = in no cluster); P <= 255, K <= 8192.
+ * cap_indptr (n+1, int64) is the reference's per-row capacity layout
+ * (indptr_linear / indptr_constant): row i keeps at most cap_indptr[i+1] -
+ * cap_indptr[i] columns -- the first ones met in processing order (the
+ * partition with the fewest clusters, then the others by index; within a
+ * partition by column) -- and the counts of the others are discarded.
+ * Three calls sharing one workspace, in this order:
+ *   eacb_coassoc_prepare: builds the cluster member lists (stable counting
+ *     sort) and the processing order; *host_max_cluster receives the largest
+ *     cluster size (MyML/MyML/EAC/sparse.py:1065, the base of max_assocs);
+ *   eacb_coassoc_count: counts the kept columns of every row, writes indptr
+ *     (n+1) and *host_nnz; returns EACB_ERR_FIRST_PARTITION_OVERFLOW where
+ *     the reference would write a first-partition row past its capacity;
+ *   eacb_coassoc_fill: writes indices (nnz, int32, ascending per row) and
+ *     data (nnz, uint8 counts, or (max count + 1) - count when make_diassoc,
+ *     MyML/MyML/EAC/sparse.py:295-311), *host_discarded (nnz_discarded) and
+ *     *host_max_count.
+ * ------------------------------------------------------------------------ */
+size_t eacb_coassoc_workspace_size(int32_t n, int32_t P, int32_t K);
+int eacb_coassoc_prepare(const int32_t *labels, int32_t n, int32_t P, int32_t K,
+                         int64_t *host_max_cluster, void *ws, size_t ws_bytes, uintptr_t stream);
+int eacb_coassoc_count(const int32_t *labels, int32_t n, int32_t P, int32_t K,
+                       const int64_t *cap_indptr, int64_t *indptr, int64_t *host_nnz,
+                       void *ws, size_t ws_bytes, uintptr_t stream);
+int eacb_coassoc_fill(const int32_t *labels, int32_t n, int32_t P, int32_t K,
+                      const int64_t *cap_indptr, const int64_t *indptr,
+                      int32_t *indices, uint8_t *data, int32_t make_diassoc,
+                      int64_t *host_discarded, int32_t *host_max_count,
+                      void *ws, size_t ws_bytes, uintptr_t stream);
+
+/* Per-row capacity layouts of the co-association rows (exclusive scan of
+ * the capacities, n+1 int64).  Replaces MyML/MyML/EAC/sparse.py:371-413
+ * (indptr_linear: max_assocs for rows below n_s*n, then the line down to
+ * val_e*max_assocs at n_e*n, in the reference's float64 arithmetic) and
+ * :368-369 (indptr_constant). */
+size_t eacb_capacity_workspace_size(int32_t n);
+int eacb_capacity_linear(int32_t n, int64_t max_assocs, double n_s, double n_e,
+                         double val_s, double val_e, int64_t *cap_indptr,
+                         void *ws, size_t ws_bytes, uintptr_t stream);
+int eacb_capacity_constant(int32_t n, int64_t max_assocs, int64_t *cap_indptr,
+                           uintptr_t stream);
+
+/* data[e] = max_val - data[e] (uint8), MyML/MyML/EAC/sparse.py:295-311
+ * (make_diassoc; the reference passes max count + 1). */
+int eacb_make_diassoc(uint8_t *data, int64_t nnz, int32_t max_val, uintptr_t stream);
+
+/* ------------------------------------------------------------------------
  * EAC final clustering of a condensed co-association dissimilarity matrix.
  * Replaces MyML/MyML/EAC/eac.py:199-267 (sp_sl_lifetime) with
  * lifetime_n_clusters :366-391, whose MST is the Kruskal of

@@ -73,3 +73,79 @@ def lifetime_n_clusters(weights):
     if th < 2 * minimum:
         cont = 1
     return cont, th
+
+
+class EAC:
+    """Evidence accumulation clustering (MyML/MyML/EAC/eac.py:40-179).
+
+    Same keyword arguments; the sparse path (``sparse=True``) is the one built
+    on the GPU.  ``buildMatrix`` accepts the reference's list-of-clusters
+    ensemble or a (P x n) label matrix (numpy or CUDA tensor)."""
+
+    def __init__(self, n_samples, **kwargs):
+        self.n_samples = n_samples
+        self.n_partitions = kwargs.get("n_partitions", 100)
+        self.iters = kwargs.get("iters", 3)
+        self.n_clusters = kwargs.get("n_clusters", "sqrt")
+        self.condensed = kwargs.get("condensed", True)
+        self.kNN = kwargs.get("kNN", False)
+        self.assoc_dtype = kwargs.get("assoc_dtype", np.uint8)
+        self.sparse = kwargs.get("sparse", False)
+        self.sp_sort = kwargs.get("sparse_sort_mode", "surgical")
+        self.sp_max_assocs = kwargs.get("sparse_max_assocs", None)
+        self.sp_max_assocs_factor = kwargs.get("sparse_max_assocs_factor", 3)
+        self.sp_max_assocs_mode = kwargs.get("sparse_max_assocs_mode", "linear")
+        self.sp_keep_degree = kwargs.get("sparse_keep_degree", False)
+        self.full = not self.sparse and not self.kNN
+        self.coassoc_store = kwargs.get("coassoc_store", False)
+        self.linkage = kwargs.get("linkage", "SL")
+        self.disk_mst = kwargs.get("sl_disk", False)
+        self.stream = kwargs.get("stream", None)
+
+    def buildMatrix(self, ensemble):
+        from .sparse import EAC_CSR, CoassocBuilder, label_matrix_from_ensemble
+        if not self.sparse:
+            raise NotImplementedError("the dense co-association path is not part of the GPU "
+                                      "build; use sparse=True")
+        if self.disk_mst or self.coassoc_store:
+            raise NotImplementedError("disk-backed storage is not part of the GPU build")
+        t = _lib.torch()
+        labels = ensemble
+        if not isinstance(ensemble, (np.ndarray, t.Tensor)):
+            labels = label_matrix_from_ensemble(ensemble, self.n_samples)
+        builder = CoassocBuilder(labels, self.n_samples, stream=self.stream)
+        if self.sp_max_assocs is None:
+            self.sp_max_assocs = builder.max_cluster * self.sp_max_assocs_factor
+        coassoc = EAC_CSR(self.n_samples, max_assocs=int(self.sp_max_assocs),
+                          condensed=self.condensed, max_assocs_type=self.sp_max_assocs_mode,
+                          sort_mode=self.sp_sort, dtype=self.assoc_dtype, stream=self.stream)
+        coassoc.update_ensemble(None, builder=builder)
+        coassoc._condense(keep_degree=self.sp_keep_degree)
+        coassoc.make_diassoc()
+        self.coassoc = coassoc
+
+    def finalClustering(self, n_clusters=0):
+        if not self.sparse:
+            raise NotImplementedError("the dense co-association path is not part of the GPU build")
+        c = self.coassoc
+        n_fclusts, labels = sp_sl_lifetime_csr(c.indptr, c.indices, c.data, self.n_samples,
+                                               self.n_partitions, n_clusters=n_clusters,
+                                               stream=self.stream)
+        self.n_fclusts = n_fclusts
+        self.labels = labels
+        return labels
+
+
+def eac_pipeline(X, n_partitions, n_clusters, iters=3, label_mode="cuda",
+                 centroid_mode="numba", factor=3, stream=None):
+    """Ensemble (batched K-Means) -> sparse co-association -> Boruvka MST ->
+    lifetime cut, all on the device.  Returns (n_fclusts, labels, eac)."""
+    from ..utils.partition import generate_ensemble_labels
+    n = int(X.shape[0])
+    L, _ = generate_ensemble_labels(X, n_clusters, n_partitions, iters, label_mode=label_mode,
+                                    centroid_mode=centroid_mode, stream=stream)
+    eac = EAC(n, sparse=True, condensed=True, n_partitions=n_partitions,
+              sparse_max_assocs_factor=factor, stream=stream)
+    eac.buildMatrix(L)
+    labels = eac.finalClustering()
+    return eac.n_fclusts, labels, eac

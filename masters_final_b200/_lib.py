@@ -47,10 +47,26 @@ def load():
         "eacb_scan_excl_i32": (ctypes.c_int, [p, p, i64, i64, p, p, sz, p]),
         "eacb_scan_excl_i32_i64": (ctypes.c_int, [p, p, i64, i64, p, p, sz, p]),
         "eacb_scan_excl_i64": (ctypes.c_int, [p, p, i64, i64, p, p, sz, p]),
+        "eacb_debug_set_rounds": (None, [ctypes.c_int]),
         "eacb_boruvka_workspace_size": (sz, [i32, i64]),
         "eacb_boruvka_mst": (ctypes.c_int, [p, p, ctypes.c_int, p, p, i32, i64, p, P64, p, sz, p]),
         "eacb_connected_components": (ctypes.c_int, [p, p, ctypes.c_int, p, p, i32, i64, p, P64,
                                                      p, sz, p]),
+        "eacb_kmeans_workspace_size": (sz, [i32, i32, i32, i32]),
+        "eacb_kmeans_ensemble": (ctypes.c_int, [p, i32, i32, i32, p, i32, p, i32, ctypes.c_float,
+                                                i32, i32, p, p, p, p, p, p, sz, p]),
+        "eacb_kmeans_label_workspace_size": (sz, [i32, i32, i32]),
+        "eacb_kmeans_label": (ctypes.c_int, [p, i32, i32, p, i32, i32, p, p, p, sz, p]),
+        "eacb_coassoc_workspace_size": (sz, [i32, i32, i32]),
+        "eacb_coassoc_prepare": (ctypes.c_int, [p, i32, i32, i32, P64, p, sz, p]),
+        "eacb_coassoc_count": (ctypes.c_int, [p, i32, i32, i32, p, p, P64, p, sz, p]),
+        "eacb_capacity_workspace_size": (sz, [i32]),
+        "eacb_capacity_linear": (ctypes.c_int, [i32, i64, ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_double, ctypes.c_double, p, p, sz, p]),
+        "eacb_capacity_constant": (ctypes.c_int, [i32, i64, p, p]),
+        "eacb_make_diassoc": (ctypes.c_int, [p, i64, i32, p]),
+        "eacb_coassoc_fill": (ctypes.c_int, [p, i32, i32, i32, p, p, p, p, i32, P64, P32, p, sz,
+                                             p]),
         "eacb_final_clustering_workspace_size": (sz, [i32, i64]),
         "eacb_final_clustering": (ctypes.c_int, [p, p, p, i32, i64, i32, i32, p, P64, P32, p, sz,
                                                  p]),

@@ -355,7 +355,10 @@ __global__ void k_emit(const unsigned long long *best, const int32_t *emit, cons
         if (emit[s]) out[pos[s]] = best[s];
 }
 
-// roots by pointer chasing with path halving; bounded (a non-forest errors)
+// roots by pointer chasing with path halving; bounded (a non-forest errors).
+// A halving step replaces c's parent p by its grandparent g only if c still
+// points at p (compare-and-swap): a plain store could overwrite the root that
+// c's own thread already stored, leaving c on a non-root.
 __global__ void k_jump(int32_t *color, int32_t V, int *err)
 {
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
@@ -366,7 +369,7 @@ __global__ void k_jump(int32_t *color, int32_t V, int *err)
             int32_t p = color[c];
             if (p == c) break;
             int32_t g = color[p];
-            if (g != p) color[c] = g;      // halving: benign race, stays an ancestor
+            if (g != p) atomicCAS(&color[c], p, g);
             c = g;
             if (++guard > (int64_t)V + 64) {
                 set_err(err, DEV_CHASE_LIMIT);
@@ -432,6 +435,7 @@ struct Engine {
     ScanScratch scan;
     int32_t V0;
     int64_t Emax;
+    int max_rounds = 96;      // lowered only by the round-trace debug entry point
 
     static Engine carve(Carver &c, int32_t V0, int64_t Emax)
     {
@@ -498,7 +502,7 @@ struct Engine {
         int64_t E = E0;
         int64_t n_mst = 0;
         uint64_t *ein = ea, *eout = eb;
-        for (int round = 0; round < 96; ++round) {
+        for (int round = 0; round < max_rounds; ++round) {
             const unsigned gv = grid_for(V, 256);
             k_select<MODE><<<gv, 256, 0, st>>>(best, succ, V, label, pk);
             EACB_CHECK_LAUNCH();
@@ -559,9 +563,16 @@ struct Engine {
             V = Vn;
             E = En;
         }
+        if (max_rounds < 96) {        // debug trace: stopped on purpose
+            *n_mst_out = n_mst;
+            *n_comp_out = V;
+            return EACB_OK;
+        }
         return EACB_ERR_NOT_CONVERGED;
     }
 };
+
+static int g_debug_rounds = 0;   // 0 = off; else rounds to run (round-trace test entry)
 
 template <typename WT>
 static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wbits,
@@ -589,6 +600,7 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
     if (s) return s;
     if ((s = g.read_counts(st, h))) return s;
     int64_t n_mst = 0, n_comp = 0;
+    if (g_debug_rounds > 0) g.max_rounds = g_debug_rounds;
     if (mode == SEL_MST) s = g.run<SEL_MST>(pk, h[0], st, &n_mst, &n_comp);
     else s = g.run<SEL_CC>(pk, h[0], st, &n_mst, &n_comp);
     if (s) return s;
@@ -605,6 +617,9 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
                                   cudaMemcpyDeviceToDevice, st));
         *host_n_comp = n_comp;
     }
+    if (g_debug_rounds > 0 && labels_out && mode == SEL_MST)
+        EACB_CUDA(cudaMemcpyAsync(labels_out, g.label, sizeof(int32_t) * V,
+                                  cudaMemcpyDeviceToDevice, st));
     return EACB_OK;
 }
 
@@ -748,6 +763,10 @@ __global__ void k_canon(const int32_t *label, const int32_t *cmin, const int32_t
 }  // namespace eacb
 
 using namespace eacb;
+
+// Test hook: the next graph calls stop after `rounds` Boruvka rounds (0 =
+// run to completion) so tests can compare per-round state.
+extern "C" void eacb_debug_set_rounds(int rounds) { g_debug_rounds = rounds; }
 
 extern "C" size_t eacb_boruvka_workspace_size(int32_t n_vertices, int64_t n_edges)
 {

@@ -1,0 +1,642 @@
+// Sparse co-association matrix (condensed CSR of co-occurrence counts).
+//
+// Reference: MyML/MyML/EAC/sparse.py -- EAC_CSR.update_ensemble :154-166,
+// update_cluster_fp_condensed :446-465 (first partition, no capacity check),
+// update_cluster_sorted_surgical_condensed :957-1040 (sorted rows, capacity
+// per row, later associations discarded), _condense :212-226.
+//
+// Semantics reproduced exactly: row i of the condensed matrix holds the
+// columns j > i that share a cluster with i in some partition, with the count
+// of such partitions.  A row keeps at most cap(i) = cap_indptr[i+1] -
+// cap_indptr[i] columns: the first cap(i) distinct columns in the order
+// (rank of the first partition where the pair co-occurs in processing order,
+// then j); counts of discarded columns are summed into nnz_discarded.  The
+// processing order is the partition with the fewest non-empty clusters
+// first (lowest index on ties), then the others by index.
+//
+// B200 design (not the reference's insertion sort into pre-allocated rows):
+//  1. per partition, cluster member lists sorted by point index are built by
+//     a stable counting sort (tile histograms, one device scan over
+//     (partition, cluster, tile), warp-level match_any placement); a point's
+//     "tail" in a partition is then the contiguous run of its cluster's
+//     member list after its own position.
+//  2. pass 1, one CTA per row (persistent, dynamic row queue): the row's P
+//     tails are streamed in column chunks into a shared-memory bitmap
+//     (atomicOr); popcounts give the exact number of distinct columns, hence
+//     the kept count min(D_i, cap(i)) and the row offsets (device scan).
+//  3. pass 2, same streaming into shared-memory byte counters (one byte per
+//     column, four packed per word), then a block-wide compaction of the
+//     non-zero counters writes the row in column order straight into the
+//     final CSR.  Rows whose distinct count exceeds their capacity (rare)
+//     are redone by a rank-aware kernel that streams partitions in
+//     processing order and applies the keep rule.
+#include "eacb_common.cuh"
+#include "scan_impl.cuh"
+#include "members.cuh"
+
+namespace eacb {
+
+constexpr int kMaxK = 8192;            // largest cluster id + 1 supported
+constexpr int kRowThreads = 512;
+constexpr int kBitmapBytes = 96 * 1024;        // pass 1: 786,432 columns per chunk
+constexpr int kCountBytes = 96 * 1024;         // pass 2: 98,304 columns per chunk
+constexpr int kCapBytes = 48 * 1024;           // capped rows: counts + ranks
+constexpr int kMaxP = 255;
+
+struct CoWS {
+    int *err;
+    int32_t *members;     // P*n, member lists of every partition, back to back
+    int32_t *mypos;       // P*n, global position of point i in its member list (-1: none)
+    int32_t *cnt;         // P*K*ntiles tile counts
+    int64_t *S;           // exclusive scan of cnt (+ total)
+    int32_t *ncl;         // P non-empty clusters
+    int32_t *order;       // P processing order
+    int32_t *rowcnt;      // n kept columns per row
+    int32_t *rowflag;     // n: 1 = distinct columns exceed the capacity
+    int *queue;           // 4 row-queue counters
+    unsigned long long *disc;   // discarded counts
+    int *maxcnt;          // largest kept count
+    ScanScratch scan;
+    int64_t ntiles;
+    static CoWS carve(Carver &c, int32_t n, int32_t P, int32_t K)
+    {
+        CoWS w;
+        w.err = c.take<int>(1);
+        w.ntiles = ((int64_t)n + kMLTile - 1) / kMLTile;
+        const int64_t pn = (int64_t)P * n;
+        const int64_t m = (int64_t)P * K * w.ntiles;
+        w.members = c.take<int32_t>(pn > 0 ? pn : 1);
+        w.mypos = c.take<int32_t>(pn > 0 ? pn : 1);
+        w.cnt = c.take<int32_t>(m + 1);
+        w.S = c.take<int64_t>(m + 1);
+        w.ncl = c.take<int32_t>(P > 0 ? P : 1);
+        w.order = c.take<int32_t>(P > 0 ? P : 1);
+        w.rowcnt = c.take<int32_t>(n);
+        w.rowflag = c.take<int32_t>(n);
+        w.queue = c.take<int>(4);
+        w.disc = c.take<unsigned long long>(1);
+        w.maxcnt = c.take<int>(1);
+        w.scan = ScanScratch::carve(c, m + 1 > n ? m + 1 : n, w.err);
+        return w;
+    }
+};
+
+// ------------------------------------------------------------- row tails --
+struct TailCtx {
+    const int32_t *labels;
+    const int32_t *members;
+    const int32_t *mypos;
+    const int64_t *S;
+    int32_t n, P, K;
+    int64_t ntiles;
+    // [start, end) of point i's tail in partition p (start == end: none)
+    __device__ void tail(int32_t i, int32_t p, int64_t &s, int64_t &e) const
+    {
+        int32_t mp = mypos[(int64_t)p * n + i];
+        if (mp < 0) { s = e = 0; return; }
+        int32_t c = labels[(int64_t)p * n + i];
+        s = (int64_t)mp + 1;
+        e = S[((int64_t)p * K + c + 1) * ntiles];
+    }
+};
+
+__device__ __forceinline__ int next_row(int *queue, int *s_row)
+{
+    if (threadIdx.x == 0) *s_row = atomicAdd(queue, 1);
+    __syncthreads();
+    int r = *s_row;
+    __syncthreads();
+    return r;
+}
+
+template <int THREADS>
+__device__ __forceinline__ int64_t block_sum(int64_t v)
+{
+    int64_t tot;
+    block_excl_sum<THREADS>(v, tot);
+    return tot;
+}
+
+// Stream the tails of all partitions into [j0, jl): calls op(j) per element.
+// Cursor ts[p] advances past consumed elements.
+template <typename Op>
+__device__ __forceinline__ void stream_chunk(const int32_t *members, int64_t *ts, const int64_t *te,
+                                             int32_t P, int32_t jl, Op op)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int p = warp; p < P; p += nw) {
+        int64_t cur = ts[p];
+        const int64_t end = te[p];
+        while (cur < end) {
+            const int64_t idx = cur + lane;
+            const int32_t j = idx < end ? members[idx] : 0x7fffffff;
+            const bool ok = j < jl;
+            const unsigned bal = __ballot_sync(0xffffffffu, ok);
+            if (ok) op(j);
+            cur += __popc(bal);
+            if (bal != 0xffffffffu) break;
+        }
+        if (lane == 0) ts[p] = cur;
+    }
+}
+
+// ---------------------------------------------------------------- pass 1 --
+__global__ void __launch_bounds__(kRowThreads)
+k_rows_count(TailCtx tc, const int32_t *order, const int64_t *cap_indptr, int32_t *rowcnt,
+             int32_t *rowflag, int *queue, int *err)
+{
+    extern __shared__ uint32_t bm[];
+    __shared__ int64_t ts[kMaxP], te[kMaxP];
+    __shared__ int s_row;
+    const int32_t n = tc.n, P = tc.P;
+    constexpr int32_t kCols = kBitmapBytes * 8;
+    while (true) {
+        const int i = next_row(queue, &s_row);
+        if (i >= n) break;
+        const int64_t cap = cap_indptr[i + 1] - cap_indptr[i];
+        for (int p = threadIdx.x; p < P; p += blockDim.x) {
+            int64_t s, e;
+            tc.tail(i, p, s, e);
+            ts[p] = s;
+            te[p] = e;
+            if (p == order[0] && e - s > cap) set_err(err, DEV_FIRST_OVERFLOW);
+        }
+        __syncthreads();
+        int64_t D = 0;
+        for (int64_t j0 = (int64_t)i + 1; j0 < n; j0 += kCols) {
+            const int32_t jl = (int32_t)((j0 + kCols < n) ? j0 + kCols : n);
+            const int nwords = (int)((jl - j0 + 31) >> 5);
+            for (int w = threadIdx.x; w < nwords; w += blockDim.x) bm[w] = 0;
+            __syncthreads();
+            const int32_t jb = (int32_t)j0;
+            stream_chunk(tc.members, ts, te, P, jl, [&](int32_t j) {
+                const int32_t o = j - jb;
+                atomicOr(&bm[o >> 5], 1u << (o & 31));
+            });
+            __syncthreads();
+            int64_t c = 0;
+            for (int w = threadIdx.x; w < nwords; w += blockDim.x) c += __popc(bm[w]);
+            D += block_sum<kRowThreads>(c);
+        }
+        if (threadIdx.x == 0) {
+            rowcnt[i] = (int32_t)(D < cap ? D : cap);
+            rowflag[i] = D > cap;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- pass 2 --
+// Block-wide ordered compaction of the non-zero byte counters of a chunk.
+// Each thread owns a contiguous 16-byte-aligned segment.
+template <typename Keep>
+__device__ __forceinline__ int64_t emit_chunk(const uint8_t *ctr, int width, int32_t jb,
+                                              int32_t *indices, uint8_t *data, int64_t out0,
+                                              Keep keep, int &maxc)
+{
+    const int nvec = (width + 15) >> 4;
+    const int per = (nvec + blockDim.x - 1) / blockDim.x;
+    const int v0 = threadIdx.x * per, v1 = min(nvec, v0 + per);
+    int mine = 0;
+    for (int v = v0; v < v1; ++v) {
+        uint4 x = reinterpret_cast<const uint4 *>(ctr)[v];
+        const uint32_t w4[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int o = v * 16 + q * 4 + b;
+                const uint32_t cnt = (w4[q] >> (8 * b)) & 255u;
+                if (cnt && o < width && keep(o, cnt)) mine++;
+            }
+    }
+    int64_t tot;
+    int64_t at = out0 + block_excl_sum<kRowThreads>(mine, tot);
+    for (int v = v0; v < v1; ++v) {
+        uint4 x = reinterpret_cast<const uint4 *>(ctr)[v];
+        const uint32_t w4[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int o = v * 16 + q * 4 + b;
+                const uint32_t cnt = (w4[q] >> (8 * b)) & 255u;
+                if (cnt && o < width && keep(o, cnt)) {
+                    indices[at] = jb + o;
+                    data[at] = (uint8_t)cnt;
+                    maxc = max(maxc, (int)cnt);
+                    at++;
+                }
+            }
+    }
+    return tot;
+}
+
+__global__ void __launch_bounds__(kRowThreads)
+k_rows_fill(TailCtx tc, const int32_t *rowflag, const int64_t *indptr, int32_t *indices,
+            uint8_t *data, int *queue, int *gmax, int *err)
+{
+    extern __shared__ uint32_t ctr32[];
+    __shared__ int64_t ts[kMaxP], te[kMaxP];
+    __shared__ int s_row;
+    const int32_t n = tc.n, P = tc.P;
+    constexpr int32_t kCols = kCountBytes;
+    int maxc = 0;
+    while (true) {
+        const int i = next_row(queue, &s_row);
+        if (i >= n) break;
+        if (rowflag[i]) continue;            // uniform across the block
+        for (int p = threadIdx.x; p < P; p += blockDim.x) {
+            int64_t s, e;
+            tc.tail(i, p, s, e);
+            ts[p] = s;
+            te[p] = e;
+        }
+        __syncthreads();
+        int64_t out = indptr[i];
+        for (int64_t j0 = (int64_t)i + 1; j0 < n; j0 += kCols) {
+            const int32_t jl = (int32_t)((j0 + kCols < n) ? j0 + kCols : n);
+            const int width = (int)(jl - j0);
+            const int nwords = (width + 15) >> 4 << 2;
+            for (int w = threadIdx.x; w < nwords; w += blockDim.x) ctr32[w] = 0;
+            __syncthreads();
+            const int32_t jb = (int32_t)j0;
+            stream_chunk(tc.members, ts, te, P, jl, [&](int32_t j) {
+                const int32_t o = j - jb;
+                atomicAdd(&ctr32[o >> 2], 1u << (8 * (o & 3)));
+            });
+            __syncthreads();
+            out += emit_chunk((const uint8_t *)ctr32, width, jb, indices, data, out,
+                              [](int, uint32_t) { return true; }, maxc);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0 && out != indptr[i + 1]) set_err(err, DEV_CAPACITY);
+    }
+    // block max -> global
+    for (int d = 16; d >= 1; d >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, d));
+    if ((threadIdx.x & 31) == 0) atomicMax(gmax, maxc);
+}
+
+// ------------------------------------------------------ rows over capacity --
+// One CTA per flagged row.  Partitions are streamed in processing order with
+// a barrier between partitions, so the first partition that touches a
+// column is its rank.
+__global__ void __launch_bounds__(kRowThreads)
+k_rows_capped(TailCtx tc, const int32_t *order, const int32_t *rowflag, const int64_t *cap_indptr,
+              const int64_t *indptr, int32_t *indices, uint8_t *data, int *queue, int *gmax,
+              unsigned long long *disc, int *err)
+{
+    extern __shared__ uint32_t sm[];
+    uint32_t *ctr32 = sm;                                  // kCapBytes counters
+    uint8_t *rank = (uint8_t *)(sm + kCapBytes / 4);       // kCapBytes ranks
+    __shared__ int64_t ts[kMaxP], te[kMaxP];
+    __shared__ int hist[kMaxP + 1];
+    __shared__ int s_row, s_rstar, s_quota, s_seen;
+    __shared__ int64_t s_end;
+    const int32_t n = tc.n, P = tc.P;
+    constexpr int32_t kCols = kCapBytes;
+    int maxc = 0;
+    while (true) {
+        const int i = next_row(queue, &s_row);
+        if (i >= n) break;
+        if (!rowflag[i]) continue;
+        const int64_t cap = cap_indptr[i + 1] - cap_indptr[i];
+        for (int q = threadIdx.x; q <= P; q += blockDim.x) hist[q] = 0;
+        int s_rs = 0, s_qt = 0;
+        int64_t out = indptr[i];
+        unsigned long long dsum = 0;
+        for (int pass = 0; pass < 2; ++pass) {
+            for (int q = threadIdx.x; q < P; q += blockDim.x) {
+                int64_t s, e;
+                tc.tail(i, order[q], s, e);
+                ts[q] = s;
+                te[q] = e;
+            }
+            if (threadIdx.x == 0) s_seen = 0;
+            __syncthreads();
+            for (int64_t j0 = (int64_t)i + 1; j0 < n; j0 += kCols) {
+                const int32_t jl = (int32_t)((j0 + kCols < n) ? j0 + kCols : n);
+                const int width = (int)(jl - j0);
+                const int nw = (width + 15) >> 4 << 2;
+                for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+                    ctr32[w] = 0;
+                    reinterpret_cast<uint32_t *>(rank)[w] = 0xffffffffu;
+                }
+                __syncthreads();
+                for (int q = 0; q < P; ++q) {
+                    // end of this partition's run inside the chunk
+                    if (threadIdx.x == 0) {
+                        int64_t lo = ts[q], hi = te[q];
+                        while (lo < hi) {
+                            int64_t mid = (lo + hi) >> 1;
+                            if (tc.members[mid] < jl) lo = mid + 1; else hi = mid;
+                        }
+                        s_end = lo;
+                    }
+                    __syncthreads();
+                    for (int64_t idx = ts[q] + threadIdx.x; idx < s_end; idx += blockDim.x) {
+                        const int32_t o = tc.members[idx] - (int32_t)j0;
+                        const uint32_t old = atomicAdd(&ctr32[o >> 2], 1u << (8 * (o & 3)));
+                        if (((old >> (8 * (o & 3))) & 255u) == 0) rank[o] = (uint8_t)q;
+                    }
+                    __syncthreads();
+                    if (threadIdx.x == 0) ts[q] = s_end;
+                    __syncthreads();
+                }
+                if (pass == 0) {
+                    for (int o = threadIdx.x; o < width; o += blockDim.x)
+                        if (rank[o] != 0xff) atomicAdd(&hist[rank[o]], 1);
+                    __syncthreads();
+                } else {
+                    // kept: rank < r*, or rank == r* among the first `quota`
+                    // such columns in column order
+                    const int nvec = (width + 15) >> 4;
+                    const int per = (nvec + blockDim.x - 1) / blockDim.x;
+                    const int o0 = threadIdx.x * per * 16, o1 = min(width, o0 + per * 16);
+                    int mystar = 0;
+                    for (int o = o0; o < o1; ++o) mystar += (rank[o] == s_rs);
+                    int64_t tstar;
+                    int64_t before = s_seen + block_excl_sum<kRowThreads>(mystar, tstar);
+                    int64_t seen = before;
+                    const uint8_t *c8 = (const uint8_t *)ctr32;
+                    int kept = 0;
+                    for (int o = o0; o < o1; ++o) {
+                        const int r = rank[o];
+                        if (r == 0xff) continue;
+                        bool k = r < s_rs || (r == s_rs && seen < s_qt);
+                        if (r == s_rs) seen++;
+                        if (k) kept++; else dsum += c8[o];
+                    }
+                    int64_t tk;
+                    int64_t at = out + block_excl_sum<kRowThreads>(kept, tk);
+                    seen = before;
+                    for (int o = o0; o < o1; ++o) {
+                        const int r = rank[o];
+                        if (r == 0xff) continue;
+                        bool k = r < s_rs || (r == s_rs && seen < s_qt);
+                        if (r == s_rs) seen++;
+                        if (k) {
+                            indices[at] = (int32_t)j0 + o;
+                            data[at] = c8[o];
+                            maxc = max(maxc, (int)c8[o]);
+                            at++;
+                        }
+                    }
+                    out += tk;
+                    __syncthreads();
+                    if (threadIdx.x == 0) s_seen += (int)tstar;
+                    __syncthreads();
+                }
+            }
+            if (pass == 0) {
+                if (threadIdx.x == 0) {
+                    int64_t cum = 0;
+                    int rs = P, qt = 0;
+                    for (int q = 0; q < P; ++q) {
+                        if (cum + hist[q] >= cap) { rs = q; qt = (int)(cap - cum); break; }
+                        cum += hist[q];
+                    }
+                    s_rstar = rs;
+                    s_quota = qt;
+                }
+                __syncthreads();
+                s_rs = s_rstar;
+                s_qt = s_quota;
+            }
+        }
+        if (threadIdx.x == 0 && out != indptr[i + 1]) set_err(err, DEV_CAPACITY);
+        for (int d = 16; d >= 1; d >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, d);
+        if ((threadIdx.x & 31) == 0 && dsum) atomicAdd(disc, dsum);
+        __syncthreads();
+    }
+    for (int d = 16; d >= 1; d >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, d));
+    if ((threadIdx.x & 31) == 0) atomicMax(gmax, maxc);
+}
+
+__global__ void k_diassoc_val(uint8_t *data, int64_t nnz, uint32_t top)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz;
+         e += (int64_t)gridDim.x * blockDim.x)
+        data[e] = (uint8_t)(top - data[e]);
+}
+
+__global__ void k_diassoc(uint8_t *data, int64_t nnz, const int *gmax)
+{
+    const uint32_t top = (uint32_t)(*gmax) + 1u;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz;
+         e += (int64_t)gridDim.x * blockDim.x)
+        data[e] = (uint8_t)(top - data[e]);
+}
+
+static int check_args(const int32_t *labels, int32_t n, int32_t P, int32_t K)
+{
+    if (!labels || n <= 0 || P <= 0 || P > kMaxP || K <= 0) return EACB_ERR_BAD_ARGUMENT;
+    if (K > kMaxK) return EACB_ERR_UNSUPPORTED;
+    if ((int64_t)P * n >= ((int64_t)1 << 31)) return EACB_ERR_UNSUPPORTED;
+    return EACB_OK;
+}
+
+static int read_err(int *err, cudaStream_t st)
+{
+    int e = 0;
+    EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EACB_CUDA(cudaStreamSynchronize(st));
+    return dev_err_to_status(e);
+}
+
+static int row_grid()
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return 2 * sms;
+}
+
+}  // namespace eacb
+
+using namespace eacb;
+
+extern "C" size_t eacb_coassoc_workspace_size(int32_t n, int32_t P, int32_t K)
+{
+    Carver c(nullptr, 0);
+    CoWS::carve(c, n, P, K);
+    return c.off;
+}
+
+extern "C" int eacb_coassoc_prepare(const int32_t *labels, int32_t n, int32_t P, int32_t K,
+                                    int64_t *host_max_cluster, void *ws, size_t ws_bytes,
+                                    uintptr_t stream)
+{
+    int s = check_args(labels, n, P, K);
+    if (s) return s;
+    if (!host_max_cluster || !ws) return EACB_ERR_BAD_ARGUMENT;
+    cudaStream_t st = as_stream(stream);
+    Carver c(ws, ws_bytes);
+    CoWS w = CoWS::carve(c, n, P, K);
+    if (c.overflow) return EACB_ERR_WORKSPACE;
+    EACB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
+    EACB_CUDA(cudaMemsetAsync(w.queue, 0, 4 * sizeof(int), st));
+    const int64_t nt = w.ntiles;
+    const int64_t m = (int64_t)P * K * nt;
+    k_ml_count<<<(unsigned)(P * nt), 256, K * sizeof(int), st>>>(labels, n, K, nt, w.cnt, w.err);
+    EACB_CHECK_LAUNCH();
+    if ((s = scan_launch<int32_t, int64_t>(w.cnt, w.S, m, 0, &w.S[m], w.scan, st))) return s;
+    const size_t place_smem = (size_t)K * (sizeof(int64_t) + sizeof(int32_t));
+    if (place_smem > 48 * 1024)
+        EACB_CUDA(cudaFuncSetAttribute(k_ml_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)place_smem));
+    k_ml_place<<<(unsigned)(P * nt), 32, place_smem, st>>>(labels, n, K, nt, w.S, w.members,
+                                                           w.mypos);
+    EACB_CHECK_LAUNCH();
+    EACB_CUDA(cudaMemsetAsync(w.maxcnt, 0, sizeof(int), st));
+    k_ncl<<<P, 256, 0, st>>>(w.S, K, nt, w.ncl, w.maxcnt);
+    EACB_CHECK_LAUNCH();
+    k_order<<<1, 32, 0, st>>>(w.ncl, P, w.order);
+    EACB_CHECK_LAUNCH();
+    int mc = 0;
+    EACB_CUDA(cudaMemcpyAsync(&mc, w.maxcnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if ((s = read_err(w.err, st))) return s;
+    *host_max_cluster = mc;
+    return EACB_OK;
+}
+
+extern "C" int eacb_coassoc_count(const int32_t *labels, int32_t n, int32_t P, int32_t K,
+                                  const int64_t *cap_indptr, int64_t *indptr, int64_t *host_nnz,
+                                  void *ws, size_t ws_bytes, uintptr_t stream)
+{
+    int s = check_args(labels, n, P, K);
+    if (s) return s;
+    if (!cap_indptr || !indptr || !host_nnz || !ws) return EACB_ERR_BAD_ARGUMENT;
+    cudaStream_t st = as_stream(stream);
+    Carver c(ws, ws_bytes);
+    CoWS w = CoWS::carve(c, n, P, K);
+    if (c.overflow) return EACB_ERR_WORKSPACE;
+    EACB_CUDA(cudaMemsetAsync(w.queue, 0, 4 * sizeof(int), st));
+    TailCtx tc{labels, w.members, w.mypos, w.S, n, P, K, w.ntiles};
+    EACB_CUDA(cudaFuncSetAttribute(k_rows_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kBitmapBytes));
+    ProfScope ps(PROF_COASSOC, st);
+    k_rows_count<<<row_grid(), kRowThreads, kBitmapBytes, st>>>(tc, w.order, cap_indptr, w.rowcnt,
+                                                                 w.rowflag, &w.queue[0], w.err);
+    EACB_CHECK_LAUNCH();
+    ps.done(0.0);
+    if ((s = scan_launch<int32_t, int64_t>(w.rowcnt, indptr, n, 0, &indptr[n], w.scan, st))) return s;
+    EACB_CUDA(cudaMemcpyAsync(host_nnz, &indptr[n], sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    return read_err(w.err, st);
+}
+
+__global__ void k_cap_linear(int32_t n, double m, double b, int64_t ns, int64_t ne, int64_t vs,
+                             int64_t ve, int64_t *y)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t v;
+        if (i < ns) v = vs;
+        else if (i < ne) v = (int64_t)__dadd_rn(__dmul_rn(m, (double)(int32_t)i), b);
+        else v = ve;
+        y[i] = v;
+    }
+}
+
+__global__ void k_cap_const(int32_t n, int64_t c, int64_t *y)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = i * c;
+}
+
+extern "C" size_t eacb_capacity_workspace_size(int32_t n)
+{
+    Carver c(nullptr, 0);
+    ScanScratch::carve(c, n);
+    c.take<int64_t>((size_t)n + 1);
+    return c.off;
+}
+
+extern "C" int eacb_capacity_linear(int32_t n, int64_t max_assocs, double n_s, double n_e,
+                                    double val_s, double val_e, int64_t *cap_indptr, void *ws,
+                                    size_t ws_bytes, uintptr_t stream)
+{
+    if (n <= 0 || max_assocs <= 0 || !cap_indptr || !ws) return EACB_ERR_BAD_ARGUMENT;
+    cudaStream_t st = as_stream(stream);
+    Carver c(ws, ws_bytes);
+    ScanScratch sc = ScanScratch::carve(c, n);
+    int64_t *y = c.take<int64_t>((size_t)n + 1);
+    if (c.overflow) return EACB_ERR_WORKSPACE;
+    // the line through (n_s*n, val_s*max) and (n_e*n, val_e*max), in the
+    // reference's float64 arithmetic (MyML/MyML/EAC/sparse.py:391-409)
+    const double fns = n_s * n, fne = n_e * n, fvs = val_s * max_assocs, fve = val_e * max_assocs;
+    const double m = (fve - fvs) / (fne - fns);
+    const double b = fvs - fns * m;
+    EACB_CUDA(cudaMemsetAsync(sc.err, 0, sizeof(int), st));
+    k_cap_linear<<<grid_for(n, 256), 256, 0, st>>>(n, m, b, (int64_t)fns, (int64_t)fne,
+                                                    (int64_t)fvs, (int64_t)fve, y);
+    EACB_CHECK_LAUNCH();
+    return scan_launch<int64_t, int64_t>(y, cap_indptr, n, 0, &cap_indptr[n], sc, st);
+}
+
+extern "C" int eacb_capacity_constant(int32_t n, int64_t max_assocs, int64_t *cap_indptr,
+                                      uintptr_t stream)
+{
+    if (n <= 0 || max_assocs <= 0 || !cap_indptr) return EACB_ERR_BAD_ARGUMENT;
+    k_cap_const<<<grid_for((int64_t)n + 1, 256), 256, 0, as_stream(stream)>>>(n, max_assocs,
+                                                                             cap_indptr);
+    EACB_CHECK_LAUNCH();
+    return EACB_OK;
+}
+
+extern "C" int eacb_make_diassoc(uint8_t *data, int64_t nnz, int32_t max_val, uintptr_t stream)
+{
+    if (nnz < 0 || (nnz > 0 && !data)) return EACB_ERR_BAD_ARGUMENT;
+    if (nnz == 0) return EACB_OK;
+    k_diassoc_val<<<grid_for(nnz, 256), 256, 0, as_stream(stream)>>>(data, nnz, (uint32_t)max_val);
+    EACB_CHECK_LAUNCH();
+    return EACB_OK;
+}
+
+extern "C" int eacb_coassoc_fill(const int32_t *labels, int32_t n, int32_t P, int32_t K,
+                                 const int64_t *cap_indptr, const int64_t *indptr,
+                                 int32_t *indices, uint8_t *data, int32_t make_diassoc,
+                                 int64_t *host_discarded, int32_t *host_max_count, void *ws,
+                                 size_t ws_bytes, uintptr_t stream)
+{
+    int s = check_args(labels, n, P, K);
+    if (s) return s;
+    if (!cap_indptr || !indptr || !host_discarded || !host_max_count || !ws)
+        return EACB_ERR_BAD_ARGUMENT;
+    cudaStream_t st = as_stream(stream);
+    Carver c(ws, ws_bytes);
+    CoWS w = CoWS::carve(c, n, P, K);
+    if (c.overflow) return EACB_ERR_WORKSPACE;
+    EACB_CUDA(cudaMemsetAsync(w.queue, 0, 4 * sizeof(int), st));
+    EACB_CUDA(cudaMemsetAsync(w.disc, 0, sizeof(unsigned long long), st));
+    EACB_CUDA(cudaMemsetAsync(w.maxcnt, 0, sizeof(int), st));
+    TailCtx tc{labels, w.members, w.mypos, w.S, n, P, K, w.ntiles};
+    EACB_CUDA(cudaFuncSetAttribute(k_rows_fill, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kCountBytes));
+    EACB_CUDA(cudaFuncSetAttribute(k_rows_capped, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   2 * kCapBytes));
+    ProfScope ps(PROF_COASSOC, st);
+    k_rows_fill<<<row_grid(), kRowThreads, kCountBytes, st>>>(tc, w.rowflag, indptr, indices, data,
+                                                               &w.queue[1], w.maxcnt, w.err);
+    EACB_CHECK_LAUNCH();
+    ps.done(0.0);
+    k_rows_capped<<<row_grid(), kRowThreads, 2 * kCapBytes, st>>>(
+        tc, w.order, w.rowflag, cap_indptr, indptr, indices, data, &w.queue[2], w.maxcnt, w.disc,
+        w.err);
+    EACB_CHECK_LAUNCH();
+    int64_t nnz = 0;
+    EACB_CUDA(cudaMemcpyAsync(&nnz, &indptr[n], sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    unsigned long long dh = 0;
+    int mh = 0;
+    EACB_CUDA(cudaMemcpyAsync(&dh, w.disc, sizeof(dh), cudaMemcpyDeviceToHost, st));
+    EACB_CUDA(cudaMemcpyAsync(&mh, w.maxcnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if ((s = read_err(w.err, st))) return s;
+    if (make_diassoc && nnz > 0) {
+        k_diassoc<<<grid_for(nnz, 256), 256, 0, st>>>(data, nnz, w.maxcnt);
+        EACB_CHECK_LAUNCH();
+    }
+    *host_discarded = (int64_t)dh;
+    *host_max_count = mh;
+    return EACB_OK;
+}

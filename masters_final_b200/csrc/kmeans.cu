@@ -1,0 +1,481 @@
+// Batched K-Means (Lloyd) ensemble generation with the reference's exact
+// arithmetic.
+//
+// Reference: MyML/MyML/cluster/KMeans.py -- fit :117-189, _init_centroids
+// :191-201, numba_label / _cu_label_kernel_dists :453-490 / :586-629,
+// numba_recompute_centroids :709-754; MyML/MyML/utils/sorting.py:9-47
+// (arg_k_select); MyML/MyML/utils/partition.py:88-124 (generateEnsemble).
+//
+// Exactness: a label is argmin_k of sum_d float64(float32((x_d - c_kd)^2))
+// with the first index winning ties, the stored distance is float32 of it,
+// centroids are float32(float64(float32 sequential sum) / count), the
+// inertia is numpy's float32 pairwise sum of the distances and a partition
+// stops early when it changes by at most tol.  The float32 label pass below
+// screens all centroids with an FMA-accumulated float32 distance and keeps
+// the best two; when the runner-up is outside the screening error bound of
+// the winner (|screen - exact| <= (D+3) 2^-23 |exact|), only the winner's
+// exact distance is computed, otherwise the point is re-labelled by the
+// exact reference loop.  The labels are therefore identical to the
+// reference's for any input.
+//
+// Batching: all P partitions of an ensemble (each with its own k) advance
+// together; every kernel takes the partition from its grid and partitions
+// that stopped early are skipped on the device.
+#include "eacb_common.cuh"
+#include "scan_impl.cuh"
+#include "members.cuh"
+#include "kmeans_common.cuh"
+
+namespace eacb {
+
+constexpr int kLT = 128;         // label threads per block
+constexpr int kLPPT = 2;         // points per thread
+constexpr int kLCH = 128;        // centroids per shared-memory chunk
+
+template <int DM>
+__global__ void __launch_bounds__(kLT)
+k_label_f32(const float *__restrict__ X, int32_t n, int32_t D, const float *__restrict__ C,
+            const int32_t *__restrict__ kk, int32_t kmax, const int32_t *__restrict__ active,
+            double ratio, int32_t *__restrict__ labels, float *__restrict__ dists,
+            int32_t *__restrict__ amb, int *__restrict__ namb)
+{
+    __shared__ float cs[kLCH * DM];
+    const int p = blockIdx.y;
+    if (!active[p]) return;
+    const int K = kk[p];
+    const float *Cp = C + (int64_t)p * kmax * D;
+    float x[kLPPT][DM];
+    float b1[kLPPT], b2[kLPPT];
+    int i1[kLPPT];
+    int64_t idx[kLPPT];
+#pragma unroll
+    for (int q = 0; q < kLPPT; ++q) {
+        idx[q] = ((int64_t)blockIdx.x * kLPPT + q) * kLT + threadIdx.x;
+#pragma unroll
+        for (int d = 0; d < DM; ++d) x[q][d] = (idx[q] < n && d < D) ? X[idx[q] * D + d] : 0.f;
+        b1[q] = b2[q] = __int_as_float(0x7f800000);
+        i1[q] = 0;
+    }
+    for (int c0 = 0; c0 < K; c0 += kLCH) {
+        const int cn = min(kLCH, K - c0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < cn * D; e += kLT) {
+            const int c = e / D, d = e - c * D;
+            cs[c * DM + d] = Cp[(int64_t)(c0 + c) * D + d];
+        }
+        __syncthreads();
+        for (int c = 0; c < cn; ++c) {
+            float s[kLPPT];
+#pragma unroll
+            for (int q = 0; q < kLPPT; ++q) s[q] = 0.f;
+#pragma unroll
+            for (int d = 0; d < DM; ++d) {
+                if (d < D) {
+                    const float cv = cs[c * DM + d];
+#pragma unroll
+                    for (int q = 0; q < kLPPT; ++q) {
+                        const float t = x[q][d] - cv;
+                        s[q] = fmaf(t, t, s[q]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kLPPT; ++q) {
+                if (s[q] < b1[q]) {
+                    b2[q] = b1[q];
+                    b1[q] = s[q];
+                    i1[q] = c0 + c;
+                } else if (s[q] < b2[q]) {
+                    b2[q] = s[q];
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kLPPT; ++q) {
+        if (idx[q] >= n) continue;
+        const int64_t o = (int64_t)p * n + idx[q];
+        if ((double)b2[q] > (double)b1[q] * ratio) {
+            labels[o] = i1[q];
+            dists[o] = (float)exact_dist<DM>(x[q], Cp + (int64_t)i1[q] * D, D);
+        } else {
+            const int slot = atomicAdd(namb, 1);
+            amb[slot] = (int32_t)o;      // resolved by k_label_exact
+        }
+    }
+}
+
+// reference loop for the points the screen could not separate
+__global__ void k_label_exact(const float *__restrict__ X, int32_t n, int32_t D,
+                              const float *__restrict__ C, const int32_t *__restrict__ kk,
+                              int32_t kmax, const int32_t *__restrict__ amb,
+                              const int *__restrict__ namb, int32_t *labels, float *dists)
+{
+    const int m = *namb;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        const int64_t o = amb[t];
+        const int64_t p = o / n, i = o - p * n;
+        const int K = kk[p];
+        const float *x = X + i * D;
+        const float *Cp = C + p * kmax * D;
+        double best = 0.0;
+        int bl = 0;
+        for (int k = 0; k < K; ++k) {
+            double dist = 0.0;
+            for (int d = 0; d < D; ++d) {
+                const float diff = __fsub_rn(x[d], Cp[(int64_t)k * D + d]);
+                dist = __dadd_rn(dist, (double)__fmul_rn(diff, diff));
+            }
+            if (k == 0 || dist < best) {
+                best = dist;
+                bl = k;
+            }
+        }
+        labels[o] = bl;
+        dists[o] = (float)best;
+    }
+}
+
+// numpy float32 add.reduce of a contiguous array: pairwise summation, blocks
+// of at most 128 summed with 8 partial sums
+__device__ __noinline__ float np_pairwise(const float *a, int64_t n)
+{
+    if (n < 8) {
+        float r = -0.0f;
+        for (int64_t i = 0; i < n; ++i) r = __fadd_rn(r, a[i]);
+        return r;
+    }
+    if (n <= 128) {
+        float r[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) r[j] = a[j];
+        int64_t i = 8;
+        for (; i < n - (n % 8); i += 8)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) r[j] = __fadd_rn(r[j], a[i + j]);
+        float res = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
+                              __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
+        for (; i < n; ++i) res = __fadd_rn(res, a[i]);
+        return res;
+    }
+    int64_t n2 = n / 2;
+    n2 -= n2 % 8;
+    return __fadd_rn(np_pairwise(a, n2), np_pairwise(a + n2, n - n2));
+}
+
+// inertia and the convergence test of one iteration (KMeans.py:158-180)
+__global__ void k_inertia(const float *dists, int32_t n, int32_t P, int32_t *active,
+                          float *inertia, int32_t *iters, float tol)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P || !active[p]) return;
+    const float I = np_pairwise(dists + (int64_t)p * n, n);
+    const float err = fabsf(__fsub_rn(I, inertia[p]));
+    inertia[p] = I;
+    iters[p] += 1;
+    if (err <= tol) active[p] = 0;
+}
+
+// float32 (reference) or float64 sums of each cluster's members in point order
+template <bool F64>
+__global__ void k_centroids(const float *__restrict__ X, int32_t n, int32_t D,
+                            const int32_t *__restrict__ members, const int64_t *__restrict__ S,
+                            int32_t K, int64_t ntiles, const int32_t *__restrict__ kk, int32_t kmax,
+                            const int32_t *__restrict__ active, float *C, int32_t *nempty)
+{
+    const int p = blockIdx.y;
+    if (!active[p]) return;
+    const int Kp = kk[p];
+    const int lane = threadIdx.x & 31;
+    const int G = 32 / D;                       // clusters per warp
+    const int g = lane / D, d = lane - g * D;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int c = warp * G + g;
+    if (g >= G || c >= Kp) return;
+    const int64_t s0 = S[((int64_t)p * K + c) * ntiles], s1 = S[((int64_t)p * K + c + 1) * ntiles];
+    const int64_t cnt = s1 - s0;
+    float *out = C + ((int64_t)p * kmax + c) * D + d;
+    if (cnt == 0) {
+        if (d == 0) atomicAdd(&nempty[p], 1);
+        return;
+    }
+    if (F64) {
+        double acc = 0.0;
+        for (int64_t m = s0; m < s1; ++m) acc += (double)X[(int64_t)members[m] * D + d];
+        *out = __double2float_rn(acc / (double)cnt);
+    } else {
+        float acc = 0.f;
+        int64_t m = s0;
+        for (; m + 4 <= s1; m += 4) {
+            const float v0 = X[(int64_t)members[m] * D + d];
+            const float v1 = X[(int64_t)members[m + 1] * D + d];
+            const float v2 = X[(int64_t)members[m + 2] * D + d];
+            const float v3 = X[(int64_t)members[m + 3] * D + d];
+            acc = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(acc, v0), v1), v2), v3);
+        }
+        for (; m < s1; ++m) acc = __fadd_rn(acc, X[(int64_t)members[m] * D + d]);
+        *out = __double2float_rn(__ddiv_rn((double)acc, (double)cnt));
+    }
+}
+
+// Empty clusters take the points arg_k_select returns for their number
+// (KMeans.py:727-750): the reference's quickselect, one thread per partition.
+__global__ void k_fill_empty(const float *X, int32_t n, int32_t D, const float *dists,
+                             const int64_t *S, int32_t K, int64_t ntiles, const int32_t *kk,
+                             int32_t kmax, const int32_t *active, const int32_t *nempty,
+                             int32_t *args_all, float *C, int *err)
+{
+    const int p = blockIdx.x;
+    if (threadIdx.x != 0 || !active[p] || nempty[p] == 0) return;
+    const int k = nempty[p];
+    const float *a = dists + (int64_t)p * n;
+    int32_t *args = args_all + (int64_t)p * n;
+    for (int64_t i = 0; i < n; ++i) args[i] = (int32_t)i;
+    int64_t lo = 0, hi = n - 1, guard = 0;
+    const int64_t limit = 64 * (int64_t)n + 4096;
+    while (lo < hi) {
+        int64_t r = lo, w = hi;
+        const float mid = a[args[(r + w) / 2]];
+        while (r < w) {
+            if (a[args[r]] >= mid) {
+                const int32_t t = args[w];
+                args[w] = args[r];
+                args[r] = t;
+                w--;
+            } else {
+                r++;
+            }
+            ++guard;
+        }
+        if (a[args[r]] > mid) r--;
+        if (k <= r) hi = r; else lo = r + 1;
+        if (++guard > limit) { set_err(err, DEV_CHASE_LIMIT); return; }
+    }
+    const int Kp = kk[p];
+    int e = 0;
+    for (int c = 0; c < Kp; ++c) {
+        if (S[((int64_t)p * K + c + 1) * ntiles] != S[((int64_t)p * K + c) * ntiles]) continue;
+        const int32_t src = args[e++];
+        for (int d = 0; d < D; ++d) C[((int64_t)p * kmax + c) * D + d] = X[(int64_t)src * D + d];
+    }
+}
+
+__global__ void k_init_centroids(const float *X, int32_t D, const int32_t *init, const int32_t *kk,
+                                 int32_t kmax, int32_t P, float *C, int32_t *active, float *inertia,
+                                 int32_t *iters, int32_t n, int *err)
+{
+    const int64_t total = (int64_t)P * kmax * D;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = e / ((int64_t)kmax * D);
+        const int64_t r = e - p * kmax * D;
+        const int c = (int)(r / D), d = (int)(r % D);
+        if (c >= kk[p]) continue;
+        const int32_t src = init[p * kmax + c];
+        if (src < 0 || src >= n) { set_err(err, DEV_BAD_INPUT); continue; }
+        C[e] = X[(int64_t)src * D + d];
+        if (c == 0 && d == 0) {
+            active[p] = 1;
+            inertia[p] = __int_as_float(0x7f800000);
+            iters[p] = 0;
+        }
+    }
+}
+
+struct KMWS {
+    int *err;
+    float *dists;
+    int32_t *active, *iters, *nempty, *amb, *namb;
+    float *inertia;
+    int32_t *members, *mypos, *cnt, *args;
+    int64_t *S;
+    int32_t *ncl, *order;
+    int *maxsize;
+    ScanScratch scan;
+    TcScratch tc;
+    int64_t ntiles;
+    static KMWS carve(Carver &c, int32_t n, int32_t D, int32_t P, int32_t kmax)
+    {
+        KMWS w;
+        w.err = c.take<int>(1);
+        const int64_t pn = (int64_t)P * n;
+        w.ntiles = ((int64_t)n + kMLTile - 1) / kMLTile;
+        const int64_t m = (int64_t)P * kmax * w.ntiles;
+        w.dists = c.take<float>(pn);
+        w.active = c.take<int32_t>(P);
+        w.iters = c.take<int32_t>(P);
+        w.nempty = c.take<int32_t>(P);
+        w.namb = c.take<int32_t>(1);
+        w.inertia = c.take<float>(P);
+        w.amb = c.take<int32_t>(pn);
+        w.members = c.take<int32_t>(pn);
+        w.mypos = c.take<int32_t>(pn);
+        w.args = c.take<int32_t>(pn);
+        w.cnt = c.take<int32_t>(m + 1);
+        w.S = c.take<int64_t>(m + 1);
+        w.ncl = c.take<int32_t>(P);
+        w.order = c.take<int32_t>(P);
+        w.maxsize = c.take<int>(1);
+        w.scan = ScanScratch::carve(c, m + 1, w.err);
+        w.tc = TcScratch::carve(c, n, D, P, kmax);
+        w.tc.err = w.err;         // tensor-core failures report through the same word
+        return w;
+    }
+};
+
+template <int DM>
+static void launch_label(dim3 grid, cudaStream_t st, const float *X, int32_t n, int32_t D,
+                         const float *C, const int32_t *kk, int32_t kmax, const int32_t *active,
+                         double ratio, int32_t *labels, float *dists, int32_t *amb, int *namb)
+{
+    k_label_f32<DM><<<grid, kLT, 0, st>>>(X, n, D, C, kk, kmax, active, ratio, labels, dists, amb,
+                                          namb);
+}
+
+int label_pass_f32(const float *X, int32_t n, int32_t D, int32_t P, const float *C,
+                   const int32_t *kk, int32_t kmax, const int32_t *active, int32_t *labels,
+                   float *dists, int32_t *amb, int *namb, cudaStream_t st)
+{
+    // |screen - exact| <= (D + 3) 2^-23 exact, so the winner is certain when
+    // the runner-up's screened distance exceeds ratio * the winner's
+    const double eps = (double)(D + 3) * ldexp(1.0, -23);
+    const double ratio = (1.0 + eps) / (1.0 - eps);
+    EACB_CUDA(cudaMemsetAsync(namb, 0, sizeof(int), st));
+    dim3 grid((unsigned)((n + kLT * kLPPT - 1) / (kLT * kLPPT)), (unsigned)P);
+    ProfScope ps(PROF_KMEANS, st);
+    if (D <= 4) launch_label<4>(grid, st, X, n, D, C, kk, kmax, active, ratio, labels, dists, amb, namb);
+    else if (D <= 8) launch_label<8>(grid, st, X, n, D, C, kk, kmax, active, ratio, labels, dists, amb, namb);
+    else if (D <= 16) launch_label<16>(grid, st, X, n, D, C, kk, kmax, active, ratio, labels, dists, amb, namb);
+    else launch_label<32>(grid, st, X, n, D, C, kk, kmax, active, ratio, labels, dists, amb, namb);
+    EACB_CHECK_LAUNCH();
+    ps.done(0.0);
+    k_label_exact<<<148 * 4, 128, 0, st>>>(X, n, D, C, kk, kmax, amb, namb, labels, dists);
+    EACB_CHECK_LAUNCH();
+    return EACB_OK;
+}
+
+}  // namespace eacb
+
+using namespace eacb;
+
+extern "C" size_t eacb_kmeans_workspace_size(int32_t n, int32_t d, int32_t P, int32_t kmax)
+{
+    Carver c(nullptr, 0);
+    KMWS::carve(c, n, d, P, kmax);
+    (void)d;
+    return c.off;
+}
+
+extern "C" int eacb_kmeans_ensemble(const float *X, int32_t n, int32_t d, int32_t P,
+                                    const int32_t *k, int32_t kmax, const int32_t *init,
+                                    int32_t max_iter, float tol, int32_t label_mode,
+                                    int32_t centroid_mode, int32_t *labels, float *centroids,
+                                    float *dists_out, int32_t *iters_out, float *inertia_out,
+                                    void *ws, size_t ws_bytes, uintptr_t stream)
+{
+    if (!X || n <= 0 || d <= 0 || P <= 0 || !k || kmax <= 0 || !init || max_iter <= 0 ||
+        !labels || !centroids || !ws)
+        return EACB_ERR_BAD_ARGUMENT;
+    if (d > 32 || kmax > 8192) return EACB_ERR_UNSUPPORTED;
+    if (label_mode != 0 && label_mode != 1) return EACB_ERR_BAD_ARGUMENT;
+    if ((int64_t)P * n >= ((int64_t)1 << 31)) return EACB_ERR_UNSUPPORTED;
+    cudaStream_t st = as_stream(stream);
+    Carver c(ws, ws_bytes);
+    KMWS w = KMWS::carve(c, n, d, P, kmax);
+    if (c.overflow) return EACB_ERR_WORKSPACE;
+    EACB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
+    k_init_centroids<<<grid_for((int64_t)P * kmax * d, 256), 256, 0, st>>>(
+        X, d, init, k, kmax, P, centroids, w.active, w.inertia, w.iters, n, w.err);
+    EACB_CHECK_LAUNCH();
+    const int64_t nt = w.ntiles;
+    const int64_t m = (int64_t)P * kmax * nt;
+    for (int it = 0;; ++it) {
+        int s;
+        if (label_mode == 1)
+            s = label_pass_tc(X, n, d, P, centroids, k, kmax, w.active, labels, w.dists, w.amb,
+                              w.namb, w.tc, st);
+        else
+            s = label_pass_f32(X, n, d, P, centroids, k, kmax, w.active, labels, w.dists, w.amb,
+                               w.namb, st);
+        if (s) return s;
+        k_inertia<<<(P + 127) / 128, 128, 0, st>>>(w.dists, n, P, w.active, w.inertia, w.iters, tol);
+        EACB_CHECK_LAUNCH();
+        if (it + 1 >= max_iter) break;
+        // centroids of the partitions still running
+        k_ml_count<<<(unsigned)(P * nt), 256, kmax * sizeof(int), st>>>(labels, n, kmax, nt, w.cnt,
+                                                                        w.err);
+        EACB_CHECK_LAUNCH();
+        if ((s = scan_launch<int32_t, int64_t>(w.cnt, w.S, m, 0, &w.S[m], w.scan, st))) return s;
+        const size_t place_smem = (size_t)kmax * (sizeof(int64_t) + sizeof(int32_t));
+        if (place_smem > 48 * 1024)
+            EACB_CUDA(cudaFuncSetAttribute(k_ml_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)place_smem));
+        k_ml_place<<<(unsigned)(P * nt), 32, place_smem, st>>>(labels, n, kmax, nt, w.S, w.members,
+                                                               w.mypos);
+        EACB_CHECK_LAUNCH();
+        EACB_CUDA(cudaMemsetAsync(w.nempty, 0, sizeof(int32_t) * P, st));
+        const int G = 32 / d;
+        const int warps = (kmax + G - 1) / G;
+        dim3 cg((unsigned)((warps * 32 + 255) / 256), (unsigned)P);
+        if (centroid_mode == 1)
+            k_centroids<true><<<cg, 256, 0, st>>>(X, n, d, w.members, w.S, kmax, nt, k, kmax,
+                                                  w.active, centroids, w.nempty);
+        else
+            k_centroids<false><<<cg, 256, 0, st>>>(X, n, d, w.members, w.S, kmax, nt, k, kmax,
+                                                   w.active, centroids, w.nempty);
+        EACB_CHECK_LAUNCH();
+        k_fill_empty<<<P, 32, 0, st>>>(X, n, d, w.dists, w.S, kmax, nt, k, kmax, w.active, w.nempty,
+                                       w.args, centroids, w.err);
+        EACB_CHECK_LAUNCH();
+    }
+    if (dists_out)
+        EACB_CUDA(cudaMemcpyAsync(dists_out, w.dists, sizeof(float) * (size_t)P * n,
+                                  cudaMemcpyDeviceToDevice, st));
+    if (iters_out)
+        EACB_CUDA(cudaMemcpyAsync(iters_out, w.iters, sizeof(int32_t) * P, cudaMemcpyDeviceToDevice,
+                                  st));
+    if (inertia_out)
+        EACB_CUDA(cudaMemcpyAsync(inertia_out, w.inertia, sizeof(float) * P,
+                                  cudaMemcpyDeviceToDevice, st));
+    int e = 0;
+    EACB_CUDA(cudaMemcpyAsync(&e, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EACB_CUDA(cudaStreamSynchronize(st));
+    return dev_err_to_status(e);
+}
+
+extern "C" int eacb_kmeans_label(const float *X, int32_t n, int32_t d, const float *C, int32_t k,
+                                 int32_t label_mode, int32_t *labels, float *dists, void *ws,
+                                 size_t ws_bytes, uintptr_t stream)
+{
+    if (!X || n <= 0 || d <= 0 || !C || k <= 0 || !labels || !dists || !ws)
+        return EACB_ERR_BAD_ARGUMENT;
+    if (d > 32) return EACB_ERR_UNSUPPORTED;
+    cudaStream_t st = as_stream(stream);
+    Carver c(ws, ws_bytes);
+    int *err = c.take<int>(1);
+    int32_t *kk = c.take<int32_t>(1);
+    int32_t *active = c.take<int32_t>(1);
+    int *namb = c.take<int>(1);
+    int32_t *amb = c.take<int32_t>(n);
+    TcScratch tc = TcScratch::carve(c, n, d, 1, k);
+    tc.err = err;
+    if (c.overflow) return EACB_ERR_WORKSPACE;
+    EACB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    k_set2<<<1, 1, 0, st>>>(kk, active, k, 1);
+    EACB_CHECK_LAUNCH();
+    if (label_mode == 1)
+        return label_pass_tc(X, n, d, 1, C, kk, k, active, labels, dists, amb, namb, tc, st);
+    return label_pass_f32(X, n, d, 1, C, kk, k, active, labels, dists, amb, namb, st);
+}
+
+extern "C" size_t eacb_kmeans_label_workspace_size(int32_t n, int32_t d, int32_t k)
+{
+    Carver c(nullptr, 0);
+    c.take<int>(1);
+    c.take<int32_t>(1);
+    c.take<int32_t>(1);
+    c.take<int>(1);
+    c.take<int32_t>(n);
+    TcScratch::carve(c, n, d, 1, k);
+    return c.off;
+}

@@ -1,0 +1,504 @@
+// K-means label pass on tcgen05 tensor cores.
+//
+// dist(x, c) = |x|^2 - 2 x.c + |c|^2 on data centred at its mean.  The dot
+// products run as ONE BF16 GEMM with FP32 accumulation in tensor memory:
+// each float32 operand is split into a BF16 high part and a BF16 low part
+// (x = xh + xl + O(2^-16 |x|)), and the K dimension concatenates
+// [xh, xh, xl] . [ch, cl, ch] so the product carries ~16 significant bits.
+// The epilogue (8 warps, one point row per thread, half the columns per
+// warp pair) reads the accumulator tile from TMEM with tcgen05.ld, forms the
+// screened distance and keeps the best two per point.  A point whose
+// runner-up lies within the error bound 2 E (|x|^2 + max|c|^2) of its winner
+// (E derived from the BF16 split and the FP32 accumulation, times 2) is
+// re-labelled by the reference's exact loop; every other point gets its
+// winner's exact reference distance.  Labels therefore equal the
+// reference's (MyML/MyML/cluster/KMeans.py:453-490) for any input.
+//
+// Shapes: M = 128 points per CTA, N <= 256 centroids per MMA tile, K = 3d
+// padded to a multiple of 16 (<= 96).  Operands are pre-arranged in global
+// memory in the UMMA K-major no-swizzle core-matrix layout (8 rows x 16
+// bytes per core matrix, LBO = 128 B along K, SBO = 128 B * K/8 along M/N),
+// so each tile is one contiguous cp.async.bulk copy into shared memory.
+// One thread issues the MMAs; TMEM holds one 128 x 256 FP32 accumulator per
+// CTA (256 columns), two CTAs per SM share the 512 columns and overlap each
+// other's MMA and epilogue.  Every wait is bounded and reports an error.
+#include "kmeans_common.cuh"
+#include <cuda_bf16.h>
+
+namespace eacb {
+
+constexpr int kTM = 128;           // points per CTA tile
+constexpr int kTN = 256;           // centroids per MMA tile
+constexpr int kTThreads = 256;     // 8 warps
+constexpr int kTmemCols = 256;
+constexpr int kWaitLimit = 1 << 26;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// bounded wait on a phase; returns false when it gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase)
+{
+    for (int i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// UMMA shared-memory descriptor, K-major, no swizzle
+__device__ __forceinline__ uint64_t umma_desc(const void *p, uint32_t lbo, uint32_t sbo)
+{
+    const uint64_t a = smem_addr(p);
+    uint64_t d = 0;
+    d |= (a >> 4) & 0x3FFFull;
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;          // descriptor version (sm_100)
+    return d;                         // base offset 0, layout type 0 (no swizzle)
+}
+
+// instruction descriptor: BF16 x BF16 -> FP32, both K-major, M x N
+__host__ __device__ constexpr uint32_t umma_idesc(int M, int N)
+{
+    return (1u << 4)                       // D format F32
+           | (1u << 7)                     // A format BF16
+           | (1u << 10)                    // B format BF16
+           | ((uint32_t)(N >> 3) << 17)    // N
+           | ((uint32_t)(M >> 4) << 24);   // M
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t idesc, uint32_t accumulate)
+{
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(
+            tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// byte offset of element (row, k) inside a blocked K-major tile with Kp columns
+__host__ __device__ __forceinline__ uint32_t core_off(int row, int k, int Kp)
+{
+    const int g = row >> 3, rr = row & 7, q = k >> 3, kk = k & 7;
+    return (uint32_t)((((g * (Kp >> 3) + q) << 3) + rr) * 16 + kk * 2);
+}
+
+// ------------------------------------------------------------ preparation --
+// data mean, float64 partials per block then a fixed-order final sum
+__global__ void k_colsum(const float *X, int32_t n, int32_t D, double *part)
+{
+    __shared__ double s[32][33];
+    const int d = threadIdx.x & 31, r = threadIdx.x >> 5;   // 256 threads: 8 row lanes
+    double acc = 0.0;
+    if (d < D)
+        for (int64_t i = (int64_t)blockIdx.x * 8 + r; i < n; i += (int64_t)gridDim.x * 8)
+            acc += (double)X[i * D + d];
+    s[r][d] = acc;
+    __syncthreads();
+    if (r == 0 && d < D) {
+        double t = 0.0;
+        for (int q = 0; q < 8; ++q) t += s[q][d];
+        part[(int64_t)blockIdx.x * 32 + d] = t;
+    }
+}
+
+__global__ void k_mean(const double *part, int nblocks, int32_t n, int32_t D, float *mu)
+{
+    const int d = threadIdx.x;
+    if (d >= D) return;
+    double t = 0.0;
+    for (int b = 0; b < nblocks; ++b) t += part[(int64_t)b * 32 + d];
+    mu[d] = (float)(t / (double)n);
+}
+
+// rows of one operand: centred, split into BF16 hi/lo, placed in the blocked
+// layout; `order` selects [hi,hi,lo] (points) or [hi,lo,hi] (centroids).
+__device__ __forceinline__ void put_row(const float *v, const float *mu, int D, int Kp, int row,
+                                       uint8_t *tile, bool point_side, float &norm)
+{
+    float nrm = 0.f;
+    for (int k = 0; k < Kp; ++k) {
+        __nv_bfloat16 b = __float2bfloat16_rn(0.f);
+        if (k < 3 * D) {
+            const int d = k % D, part = k / D;
+            const float xc = __fsub_rn(v[d], mu[d]);
+            const __nv_bfloat16 hi = __float2bfloat16_rn(xc);
+            const __nv_bfloat16 lo = __float2bfloat16_rn(__fsub_rn(xc, __bfloat162float(hi)));
+            const bool use_lo = point_side ? (part == 2) : (part == 1);
+            b = use_lo ? lo : hi;
+            if (part == 0) nrm = fmaf(xc, xc, nrm);
+        }
+        *reinterpret_cast<__nv_bfloat16 *>(tile + core_off(row, k, Kp)) = b;
+    }
+    norm = nrm;
+}
+
+__global__ void k_prep_points(const float *X, int32_t n, int32_t D, int32_t Kp, const float *mu,
+                              uint8_t *A, float *nx, int64_t n_pad)
+{
+    const int64_t tile_bytes = (int64_t)kTM * Kp * 2;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        uint8_t *tile = A + (i / kTM) * tile_bytes;
+        float v[32];
+        for (int d = 0; d < D; ++d) v[d] = i < n ? X[i * D + d] : mu[d];
+        float nrm;
+        put_row(v, mu, D, Kp, (int)(i % kTM), tile, true, nrm);
+        nx[i] = nrm;
+    }
+}
+
+__global__ void k_prep_centroids(const float *C, const int32_t *kk, int32_t kmax, int32_t P,
+                                 int32_t D, int32_t Kp, int32_t kt_max, const float *mu,
+                                 const int32_t *active, uint8_t *B, float *nc, float *cmax2)
+{
+    const int64_t tile_bytes = (int64_t)kTN * Kp * 2;
+    const int64_t per_p = (int64_t)kt_max * kTN;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)P * per_p;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int p = (int)(e / per_p);
+        if (!active[p]) continue;
+        const int c = (int)(e % per_p);
+        uint8_t *tile = B + ((int64_t)p * kt_max + c / kTN) * tile_bytes;
+        float v[32];
+        const bool real = c < kk[p];
+        for (int d = 0; d < D; ++d) v[d] = real ? C[((int64_t)p * kmax + c) * D + d] : mu[d];
+        float nrm;
+        put_row(v, mu, D, Kp, c % kTN, tile, false, nrm);
+        nc[e] = real ? nrm : __int_as_float(0x7f800000);
+        if (real) atomicMax(reinterpret_cast<int *>(&cmax2[p]), __float_as_int(nrm));
+    }
+}
+
+// ---------------------------------------------------------------- labels --
+__global__ void __launch_bounds__(kTThreads, 2)
+k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const float *__restrict__ C,
+           const int32_t *__restrict__ kk, int32_t kmax, int32_t kt_max,
+           const int32_t *__restrict__ active, const uint8_t *__restrict__ A,
+           const float *__restrict__ nx, const uint8_t *__restrict__ B,
+           const float *__restrict__ nc, const float *__restrict__ cmax2, float E,
+           int32_t *labels, float *dists, int32_t *amb, int *namb, int *err)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t bar_a, bar_b[2], bar_mma;
+    __shared__ uint32_t tmem_slot;
+    __shared__ float s_b1[kTM], s_b2[kTM];
+    __shared__ int s_i1[kTM];
+    __shared__ int s_fail;
+    const int p = blockIdx.y;
+    if (!active[p]) return;
+    const int K = kk[p];
+    const int tiles = (K + kTN - 1) / kTN;
+    const uint32_t a_bytes = (uint32_t)kTM * Kp * 2, b_bytes = (uint32_t)kTN * Kp * 2;
+    uint8_t *sA = smem;
+    uint8_t *sB[2] = {smem + a_bytes, smem + a_bytes + b_bytes};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t tile0 = blockIdx.x;
+    const uint8_t *Ap = A + tile0 * a_bytes;
+    const uint8_t *Bp = B + (int64_t)p * kt_max * b_bytes;
+
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        mbar_init(&bar_a, 1);
+        mbar_init(&bar_b[0], 1);
+        mbar_init(&bar_b[1], 1);
+        mbar_init(&bar_mma, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_addr(&tmem_slot)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(&bar_a, a_bytes);
+        bulk_g2s(sA, Ap, a_bytes, &bar_a);
+        mbar_expect_tx(&bar_b[0], b_bytes);
+        bulk_g2s(sB[0], Bp, b_bytes, &bar_b[0]);
+    }
+    // epilogue ownership: row = 32*(warp%4) + lane, columns [128*(warp/4), +128)
+    const int row = 32 * (warp & 3) + lane;
+    const int colh = 128 * (warp >> 2);
+    const int64_t i = tile0 * kTM + row;
+    const float xn = (i < n) ? nx[i] : 0.f;
+    float b1 = __int_as_float(0x7f800000), b2 = b1;
+    int i1 = 0;
+    const uint32_t lbo = 128, sbo = 128u * (uint32_t)(Kp >> 3);
+    uint32_t ph_b[2] = {0, 0}, ph_mma = 0;
+    bool ok = true;
+    for (int t = 0; t < tiles && ok; ++t) {
+        const int buf = t & 1;
+        const int nvalid = min(kTN, K - t * kTN);
+        const int N = (nvalid + 15) & ~15;
+        if (threadIdx.x == 0) {
+            bool got = (t == 0 ? mbar_wait(&bar_a, 0) : true) && mbar_wait(&bar_b[buf], ph_b[buf]);
+            if (!got) {
+                set_err(err, DEV_SPIN_LIMIT);
+                s_fail = 1;
+            } else {
+                tc_fence_after();
+                const uint32_t idesc = umma_idesc(kTM, N);
+                for (int s = 0; s < (Kp >> 4); ++s) {
+                    const uint64_t ad = umma_desc(sA + s * 256, lbo, sbo);
+                    const uint64_t bd = umma_desc(sB[buf] + s * 256, lbo, 128u * (uint32_t)(Kp >> 3));
+                    mma_bf16(tmem, ad, bd, idesc, s > 0 ? 1u : 0u);
+                }
+                mma_commit(&bar_mma);
+                if (t + 1 < tiles) {
+                    // the other buffer's last reader (MMA of tile t-1) completed
+                    mbar_expect_tx(&bar_b[buf ^ 1], b_bytes);
+                    bulk_g2s(sB[buf ^ 1], Bp + (int64_t)(t + 1) * b_bytes, b_bytes, &bar_b[buf ^ 1]);
+                }
+            }
+        }
+        ph_b[buf] ^= 1;
+        __syncthreads();
+        if (s_fail) { ok = false; break; }
+        if (!mbar_wait(&bar_mma, ph_mma)) {
+            set_err(err, DEV_SPIN_LIMIT);
+            s_fail = 1;
+        }
+        ph_mma ^= 1;
+        tc_fence_after();
+        const float *ncp = nc + ((int64_t)p * kt_max + t) * kTN;
+        const int c_lo = colh, c_hi = min(colh + 128, nvalid);
+        for (int c0 = c_lo; c0 < c_hi; c0 += 16) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c0, v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int c = c0 + j;
+                const float s = fmaf(-2.f, v[j], xn + __ldg(&ncp[c]));   // ncp[c] = +inf past K
+                const bool lt = s < b1;
+                b2 = lt ? b1 : fminf(b2, s);
+                i1 = lt ? t * kTN + c : i1;
+                b1 = lt ? s : b1;
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+        if (s_fail) ok = false;
+    }
+    // merge the two column halves of each row
+    if (warp >= 4) {
+        s_b1[row] = b1;
+        s_b2[row] = b2;
+        s_i1[row] = i1;
+    }
+    __syncthreads();
+    if (warp < 4 && ok && i < n) {
+        const float o1 = s_b1[row], o2 = s_b2[row];
+        const int oi = s_i1[row];
+        // the lower index wins equal screened values; equal values are a
+        // near tie anyway and go to the exact re-check below
+        float w1, w2;
+        int wi;
+        if (o1 < b1) { w1 = o1; wi = oi; w2 = fminf(b1, o2); }
+        else { w1 = b1; wi = i1; w2 = fminf(o1, b2); }
+        const float bound = 2.f * E * (xn + cmax2[p]);
+        const int64_t o = (int64_t)p * n + i;
+        if (w2 - w1 > 2.f * bound) {
+            float xv[32];
+            for (int d = 0; d < D; ++d) xv[d] = X[i * D + d];
+            labels[o] = wi;
+            dists[o] = (float)exact_dist<32>(xv, C + ((int64_t)p * kmax + wi) * D, D);
+        } else {
+            amb[atomicAdd(namb, 1)] = (int32_t)o;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTmemCols));
+}
+
+__device__ __forceinline__ void exact_label_point(const float *__restrict__ X, int32_t n, int32_t D,
+                                                  const float *__restrict__ C,
+                                                  const int32_t *__restrict__ kk, int32_t kmax,
+                                                  int64_t o, int32_t *labels, float *dists)
+{
+    const int64_t p = o / n, i = o - p * n;
+    const int K = kk[p];
+    const float *x = X + i * D;
+    const float *Cp = C + p * kmax * D;
+    double best = 0.0;
+    int bl = 0;
+    for (int k = 0; k < K; ++k) {
+        double dist = 0.0;
+        for (int d = 0; d < D; ++d) {
+            const float diff = __fsub_rn(x[d], Cp[(int64_t)k * D + d]);
+            dist = __dadd_rn(dist, (double)__fmul_rn(diff, diff));
+        }
+        if (k == 0 || dist < best) {
+            best = dist;
+            bl = k;
+        }
+    }
+    labels[o] = bl;
+    dists[o] = (float)best;
+}
+
+// if a tile gave up waiting, relabel every active point with the exact loop
+// (never expected; keeps the result correct and the error reported)
+__global__ void k_exact_all(const float *__restrict__ X, int32_t n, int32_t D,
+                            const float *__restrict__ C, const int32_t *__restrict__ kk,
+                            int32_t kmax, int32_t P, const int32_t *active, const int *err,
+                            int32_t *labels, float *dists)
+{
+    if (*err == 0) return;
+    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < (int64_t)P * n;
+         o += (int64_t)gridDim.x * blockDim.x)
+        if (active[o / n]) exact_label_point(X, n, D, C, kk, kmax, o, labels, dists);
+}
+
+__global__ void k_label_exact_tc(const float *__restrict__ X, int32_t n, int32_t D,
+                                 const float *__restrict__ C, const int32_t *__restrict__ kk,
+                                 int32_t kmax, int32_t P, const int32_t *__restrict__ amb,
+                                 const int *__restrict__ namb, const int *__restrict__ err,
+                                 int32_t *labels, float *dists)
+{
+    if (*err != 0) return;                      // k_exact_all did every point
+    const int64_t cap = (int64_t)P * n;
+    const int m = (int)min((int64_t)*namb, cap);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        exact_label_point(X, n, D, C, kk, kmax, amb[t], labels, dists);
+    }
+}
+
+size_t tc_scratch_bytes(int32_t n, int32_t D, int32_t P, int32_t kmax)
+{
+    Carver c(nullptr, 0);
+    TcScratch::carve(c, n, D, P, kmax);
+    return c.off;
+}
+
+TcScratch TcScratch::carve(Carver &c, int32_t n, int32_t D, int32_t P, int32_t kmax)
+{
+    TcScratch s;
+    s.Kp = ((3 * D + 15) / 16) * 16;
+    s.n_pad = ((int64_t)n + kTM - 1) / kTM * kTM;
+    s.kt_max = (kmax + kTN - 1) / kTN;
+    s.A = c.take<uint8_t>((size_t)s.n_pad * s.Kp * 2);
+    s.nx = c.take<float>((size_t)s.n_pad);
+    s.B = c.take<uint8_t>((size_t)P * s.kt_max * kTN * s.Kp * 2);
+    s.nc = c.take<float>((size_t)P * s.kt_max * kTN);
+    s.cmax2 = c.take<float>((size_t)P);
+    s.mu = c.take<float>(32);
+    s.part = c.take<double>((size_t)32 * 296);
+    s.err = c.take<int>(1);
+    s.points_ready = false;
+    return s;
+}
+
+int label_pass_tc(const float *X, int32_t n, int32_t D, int32_t P, const float *C,
+                  const int32_t *kk, int32_t kmax, const int32_t *active, int32_t *labels,
+                  float *dists, int32_t *amb, int *namb, TcScratch &s, cudaStream_t st)
+{
+    if (!s.points_ready) {
+        k_colsum<<<296, 256, 0, st>>>(X, n, D, s.part);
+        EACB_CHECK_LAUNCH();
+        k_mean<<<1, 32, 0, st>>>(s.part, 296, n, D, s.mu);
+        EACB_CHECK_LAUNCH();
+        k_prep_points<<<grid_for(s.n_pad, 128), 128, 0, st>>>(X, n, D, s.Kp, s.mu, s.A, s.nx,
+                                                              s.n_pad);
+        EACB_CHECK_LAUNCH();
+        s.points_ready = true;
+    }
+    EACB_CUDA(cudaMemsetAsync(s.cmax2, 0, sizeof(float) * P, st));
+    EACB_CUDA(cudaMemsetAsync(namb, 0, sizeof(int), st));
+    k_prep_centroids<<<grid_for((int64_t)P * s.kt_max * kTN, 128), 128, 0, st>>>(
+        C, kk, kmax, P, D, s.Kp, s.kt_max, s.mu, active, s.B, s.nc, s.cmax2);
+    EACB_CHECK_LAUNCH();
+    // error model of the screened distance, doubled for margin: BF16 split
+    // (3 * 2^-16), FP32 accumulation over 3D products (3D * 2^-23), the
+    // norms and the epilogue arithmetic ((D + 6) * 2^-24)
+    const float E = 2.f * (float)(3.0 * ldexp(1.0, -16) + 3.0 * D * ldexp(1.0, -23) +
+                                  (D + 6) * ldexp(1.0, -24));
+    const size_t smem = (size_t)kTM * s.Kp * 2 + 2 * (size_t)kTN * s.Kp * 2;
+    // at least 100 KB so that no more than two CTAs (2 x 256 TMEM columns)
+    // share an SM
+    const size_t smem_req = smem < 100 * 1024 ? 100 * 1024 : smem;
+    EACB_CUDA(cudaFuncSetAttribute(k_label_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem_req));
+    dim3 grid((unsigned)(s.n_pad / kTM), (unsigned)P);
+    ProfScope ps(PROF_KMEANS, st);
+    k_label_tc<<<grid, kTThreads, smem_req, st>>>(X, n, D, s.Kp, C, kk, kmax, s.kt_max, active,
+                                                  s.A, s.nx, s.B, s.nc, s.cmax2, E, labels, dists,
+                                                  amb, namb, s.err);
+    EACB_CHECK_LAUNCH();
+    ps.done(0.0);
+    k_exact_all<<<296, 256, 0, st>>>(X, n, D, C, kk, kmax, P, active, s.err, labels, dists);
+    EACB_CHECK_LAUNCH();
+    k_label_exact_tc<<<148 * 4, 128, 0, st>>>(X, n, D, C, kk, kmax, P, amb, namb, s.err, labels,
+                                              dists);
+    EACB_CHECK_LAUNCH();
+    return EACB_OK;
+}
+
+}  // namespace eacb

@@ -28,6 +28,7 @@ static int scan_entry(const TIn *in, TOut *out, int64_t n, int64_t init, int64_t
     Carver c(ws, ws_bytes);
     ScanScratch s = ScanScratch::carve(c, n);
     if (c.overflow) return EACB_ERR_WORKSPACE;
+    if (n > 0) EACB_CUDA(cudaMemsetAsync(s.err, 0, sizeof(int), as_stream(stream)));
     ProfScope ps(PROF_SCAN, as_stream(stream));
     int st = scan_launch<TIn, TOut>(in, out, n, init, d_total, s, as_stream(stream));
     ps.done((double)n * (sizeof(TIn) + sizeof(TOut)));

@@ -1,0 +1,132 @@
+"""GPU parity of the sparse co-association build (EAC_CSR) against the
+reference's outputs and the oracle."""
+import hashlib
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def T():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _build(L, n, max_assocs, kind="linear"):
+    from masters_final_b200.EAC.sparse import EAC_CSR
+    c = EAC_CSR(n, int(max_assocs), max_assocs_type=kind, condensed=True, sort_mode="surgical")
+    c.update_ensemble(L)
+    return c
+
+
+@pytest.mark.parametrize("name", ["eac_small", "eac_discard"])
+def test_coassoc_golden(T, name):
+    g = golden(name)
+    n = g["x"].shape[0]
+    c = _build(g["labels_matrix"], n, g["max_assocs"])
+    assert c.nnz == g["nnz"]
+    assert c.nnz_discarded == g["nnz_discarded"]
+    c.make_diassoc()
+    assert np.array_equal(c.indptr.cpu().numpy(), g["indptr"])
+    assert np.array_equal(c.indices.cpu().numpy(), g["indices"])
+    assert np.array_equal(c.data.cpu().numpy(), g["diassoc"])
+
+
+def test_coassoc_10k_golden(T):
+    g = golden("eac_10k")
+    n = g["x"].shape[0]
+    L = g["labels_matrix"].astype(np.int32)
+    c = _build(L, n, g["max_assocs"])
+    assert c.nnz == g["nnz"] and c.nnz_discarded == g["nnz_discarded"]
+    c.make_diassoc()
+    h = hashlib.sha256()
+    for a in (c.indptr.cpu().numpy(), c.indices.cpu().numpy(), c.data.cpu().numpy()):
+        h.update(np.ascontiguousarray(a).tobytes())
+    assert h.hexdigest() == str(g["coassoc_sha"])
+
+
+def _random_labels(rng, P, n, kmin, kmax, holes=0.0):
+    L = np.empty((P, n), dtype=np.int32)
+    for p in range(P):
+        k = int(rng.integers(kmin, kmax + 1))
+        L[p] = rng.integers(0, k, n)
+        if holes:
+            L[p][rng.random(n) < holes] = -1
+    return L
+
+
+@pytest.mark.parametrize("seed,n,P,kmin,kmax,factor,kind,holes", [
+    (1, 3000, 20, 5, 40, 3, "linear", 0.0),
+    (2, 5000, 37, 2, 9, 1, "linear", 0.0),          # tight: discards
+    (3, 4000, 12, 30, 300, 2, "constant", 0.05),    # -1 labels, constant caps
+    (4, 200_000, 6, 3000, 4000, 3, "linear", 0.0),  # several column chunks per row
+    (5, 2500, 255, 10, 20, 3, "linear", 0.0),       # maximum ensemble size
+])
+def test_coassoc_vs_oracle(T, seed, n, P, kmin, kmax, factor, kind, holes):
+    rng = np.random.default_rng(seed)
+    L = _random_labels(rng, P, n, kmin, kmax, holes)
+    ma = oracle.max_cluster_size(L) * factor
+    cap = oracle.indptr_linear(n, ma) if kind == "linear" else oracle.indptr_constant(n, ma)
+    ip, ind, cnt, nnz, disc, st = oracle.coassoc_build(L, cap)
+    if st == oracle.ERR_FIRST_OVERFLOW:
+        from masters_final_b200.EAC.sparse import EAC_CSR
+        with pytest.raises(ValueError):
+            _build(L, n, ma, kind)
+        return
+    assert st == 0
+    c = _build(L, n, ma, kind)
+    assert c.nnz == nnz and c.nnz_discarded == disc
+    assert np.array_equal(c.indptr.cpu().numpy(), ip)
+    assert np.array_equal(c.indices.cpu().numpy(), ind)
+    assert np.array_equal(c.data.cpu().numpy(), cnt)
+
+
+def test_first_partition_overflow_raises(T):
+    from masters_final_b200.EAC.sparse import EAC_CSR
+    n = 1000
+    L = np.zeros((3, n), dtype=np.int32)          # one cluster holding everything
+    L[1] = np.arange(n) % 7
+    L[2] = np.arange(n) % 5
+    cap_small = 10
+    st = oracle.coassoc_build(L, oracle.indptr_constant(n, cap_small))[-1]
+    assert st == oracle.ERR_FIRST_OVERFLOW
+    with pytest.raises(ValueError):
+        _build(L, n, cap_small, "constant")
+
+
+@pytest.mark.parametrize("kind", ["linear", "constant"])
+def test_coassoc_checksum_full_size(T, kind):
+    """n = 500,000 points, 20 partitions with k in [350, 710] (the size of the
+    BF16 workload, fewer partitions).  Every co-clustered pair is either
+    counted in a kept entry or in nnz_discarded (random labels overflow the
+    linear capacities, so most rows take the capped path; a constant capacity
+    of n keeps everything); rows are strictly increasing and every column
+    exceeds its row."""
+    rng = np.random.default_rng(9)
+    n, P = 500_000, 20
+    L = _random_labels(rng, P, n, 350, 710)
+    pairs = 0
+    for p in range(P):
+        s = np.bincount(L[p]).astype(np.int64)
+        pairs += int((s * (s - 1) // 2).sum())
+    ma = oracle.max_cluster_size(L) * 3 if kind == "linear" else n
+    c = _build(L, n, ma, kind)
+    if kind == "constant":
+        assert c.nnz_discarded == 0
+    ip = c.indptr.cpu().numpy()
+    ind = c.indices.cpu().numpy()
+    dat = c.data.cpu().numpy()
+    assert int(dat.astype(np.int64).sum()) + c.nnz_discarded == pairs
+    rows = np.repeat(np.arange(n), np.diff(ip))
+    assert np.all(ind > rows)
+    same = rows[1:] == rows[:-1]
+    assert np.all(ind[1:][same] > ind[:-1][same])
+    if kind == "linear":
+        cap = oracle.indptr_linear(n, ma)
+        assert np.all(np.diff(ip) <= np.diff(cap))
