@@ -137,30 +137,67 @@ __global__ void k_label_exact(const float *__restrict__ X, int32_t n, int32_t D,
 }
 
 // numpy float32 add.reduce of a contiguous array: pairwise summation, blocks
-// of at most 128 summed with 8 partial sums
-__device__ __noinline__ float np_pairwise(const float *a, int64_t n)
+// of at most 128 summed with 8 partial sums; a node longer than 128 splits at
+// n/2 rounded down to a multiple of 8 and adds (left, right).
+__device__ __forceinline__ float np_pairwise_leaf(const float *a, int64_t n)
 {
     if (n < 8) {
         float r = -0.0f;
         for (int64_t i = 0; i < n; ++i) r = __fadd_rn(r, a[i]);
         return r;
     }
-    if (n <= 128) {
-        float r[8];
+    float r[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) r[j] = a[j];
-        int64_t i = 8;
-        for (; i < n - (n % 8); i += 8)
+    for (int j = 0; j < 8; ++j) r[j] = a[j];
+    int64_t i = 8;
+    for (; i < n - (n % 8); i += 8)
 #pragma unroll
-            for (int j = 0; j < 8; ++j) r[j] = __fadd_rn(r[j], a[i + j]);
-        float res = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
-                              __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
-        for (; i < n; ++i) res = __fadd_rn(res, a[i]);
-        return res;
+        for (int j = 0; j < 8; ++j) r[j] = __fadd_rn(r[j], a[i + j]);
+    float res = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
+                          __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
+    for (; i < n; ++i) res = __fadd_rn(res, a[i]);
+    return res;
+}
+
+// Iterative post-order walk of the split tree (depth < 48 for any int64 n),
+// so no device stack is needed.
+__device__ float np_pairwise(const float *a, int64_t n)
+{
+    int64_t off[48], len[48];
+    float left[48];
+    int stage[48];
+    int sp = 0;
+    off[0] = 0;
+    len[0] = n;
+    stage[0] = 0;
+    float ret = 0.f;
+    while (sp >= 0) {
+        if (len[sp] <= 128) {
+            ret = np_pairwise_leaf(a + off[sp], len[sp]);
+            sp--;
+            continue;
+        }
+        int64_t n2 = len[sp] / 2;
+        n2 -= n2 % 8;
+        if (stage[sp] == 0) {
+            stage[sp] = 1;
+            off[sp + 1] = off[sp];
+            len[sp + 1] = n2;
+            stage[sp + 1] = 0;
+            sp++;
+        } else if (stage[sp] == 1) {
+            left[sp] = ret;
+            stage[sp] = 2;
+            off[sp + 1] = off[sp] + n2;
+            len[sp + 1] = len[sp] - n2;
+            stage[sp + 1] = 0;
+            sp++;
+        } else {
+            ret = __fadd_rn(left[sp], ret);
+            sp--;
+        }
     }
-    int64_t n2 = n / 2;
-    n2 -= n2 % 8;
-    return __fadd_rn(np_pairwise(a, n2), np_pairwise(a + n2, n - n2));
+    return ret;
 }
 
 // inertia and the convergence test of one iteration (KMeans.py:158-180)
