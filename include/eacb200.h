@@ -85,6 +85,24 @@ int eacb_scan_excl_i32_i64(const int32_t *in, int64_t *out, int64_t n, int64_t i
 int eacb_scan_excl_i64(const int64_t *in, int64_t *out, int64_t n, int64_t init,
                        int64_t *d_total, void *ws, size_t ws_bytes, uintptr_t stream);
 
+/* Allocation-free variant of eacb_scan_excl_i32 (no counterpart in the
+ * reference).  For callers that may not allocate device memory while they
+ * run -- a host with pools fixed at start-up, a real-time path that forbids
+ * allocation, a plugin handed raw buffers and no allocator -- and so cannot
+ * supply the workspace eacb_scan_excl_i32 needs.  Same inputs, outputs and
+ * wrap-around as eacb_scan_excl_i32, no workspace argument: the look-back
+ * scratch is a fixed array of about 512 KiB in the library's device image,
+ * held on every GPU that loads the library until the process exits.  n may
+ * not exceed EACB_SCAN_NOALLOC_MAX_N (returns EACB_ERR_WORKSPACE beyond it).
+ * The first call on each device looks up that array's address
+ * (cudaGetSymbolAddress; make this first call before any stream capture).
+ * Calls share the array: calls that overlap on the GPU race, so serialise
+ * them.  The call waits for the scan to finish and returns its device-side
+ * status. */
+#define EACB_SCAN_NOALLOC_MAX_N (((int64_t)1) << 28)
+int eacb_scan_excl_i32_noalloc(const int32_t *in, int32_t *out, int64_t n, int64_t init,
+                               int64_t *d_total, uintptr_t stream);
+
 /* ------------------------------------------------------------------------
  * Boruvka minimum spanning forest of a symmetric CSR graph.
  * Replaces MyML/MyML/graph/mst.py:417-564 (boruvka_minho_gpu) and its
