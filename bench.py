@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--no-eac", action="store_true",
+                    help="skip the EAC end-to-end measurements added to the line")
     return ap.parse_args()
 
 
@@ -290,10 +292,84 @@ def run_ours(args):
                 "clocks": clk.summary()}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(indptr, dest, w, n_edges)
+        if world == 1 and not args.no_eac:
+            line["eac"] = eac_measurements(args)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# EAC end to end (ensemble -> co-association -> Boruvka MST -> lifetime cut)
+EAC_WORKLOADS = {
+    # n points, d, mixture components, partitions, k range (np.random.randint,
+    # upper bound exclusive), anisotropic, centre range, sigma, seed
+    "eac_10k_2d_100p": dict(n=10_000, d=2, comps=6, P=100, k=(50, 101), aniso=False,
+                            cr=10.0, sigma=1.0, seed=0),
+    "eac_500k_16d_200p": dict(n=500_000, d=16, comps=50, P=200, k=(350, 711), aniso=True,
+                              cr=20.0, sigma=1.0, seed=3),
+}
+
+
+def eac_run_once(X, cfg, mode, torch):
+    """One full EAC pipeline on device-resident data; per-stage CUDA events."""
+    import random
+    from masters_final_b200.utils.partition import generate_ensemble_labels
+    from masters_final_b200.EAC.eac import EAC
+    np.random.seed(cfg["seed"])
+    random.seed(cfg["seed"])
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record()
+    L, _ = generate_ensemble_labels(X, list(cfg["k"]), cfg["P"], 3, label_mode=mode)
+    ev[1].record()
+    e = EAC(cfg["n"], sparse=True, condensed=True, n_partitions=cfg["P"])
+    e.buildMatrix(L)
+    ev[2].record()
+    labels = e.finalClustering()
+    ev[3].record()
+    ev[3].synchronize()
+    ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(3)]
+    return ms, labels, e
+
+
+def eac_measurements(args):
+    """EAC points/s of the BF16 tensor-core and the FP32 pipelines on the
+    10k-point (reference CPU-runnable) and 500k-point workloads; both
+    pipelines must produce identical final partitions."""
+    import torch
+    from masters_final_b200 import workloads as W
+    out = {}
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    for name, cfg in EAC_WORKLOADS.items():
+        x = W.gaussian_mixture(cfg["n"], cfg["d"], cfg["comps"], seed=cfg["seed"],
+                               sigma=cfg["sigma"], center_range=cfg["cr"],
+                               anisotropic=cfg["aniso"])
+        X = torch.from_numpy(x).cuda()
+        small = cfg["n"] <= 50_000
+        warm, steps = (3, 5) if small else (1, 1)
+        res = {}
+        parts = {}
+        for mode in ("bf16", "cuda"):
+            for _ in range(warm):
+                eac_run_once(X, cfg, mode, torch)
+            tot = [0.0, 0.0, 0.0]
+            for _ in range(steps):
+                flush.fill_(1)
+                ms, labels, e = eac_run_once(X, cfg, mode, torch)
+                tot = [a + b for a, b in zip(tot, ms)]
+            total_ms = sum(tot) / steps
+            key = "bf16_tc" if mode == "bf16" else "fp32"
+            res[key] = {"points_per_s": cfg["n"] / (total_ms / 1000.0), "ms": total_ms,
+                        "ms_ensemble": tot[0] / steps, "ms_coassoc": tot[1] / steps,
+                        "ms_mst_cut": tot[2] / steps}
+            parts[key] = labels
+        res["identical_partitions"] = bool(np.array_equal(parts["bf16_tc"], parts["fp32"]))
+        res["nnz"] = int(e.coassoc.nnz)
+        res["nnz_discarded"] = int(e.coassoc.nnz_discarded)
+        res["n_fclusts"] = int(e.n_fclusts)
+        res["config"] = {k: (list(v) if isinstance(v, tuple) else v) for k, v in cfg.items()}
+        out[name] = res
+    return out
 
 
 def main():

@@ -112,16 +112,23 @@ constexpr int kEI = 8;     // edges per thread (striped): 2048 edges per tile
 constexpr int64_t kETile = (int64_t)kET * kEI;
 
 // Edge sources for the tile kernel ------------------------------------------
-// (a) filtering pass over the current edge array
+// Each source splits an edge into fetch() (independent global loads, issued
+// for all items of a thread before any is used) and resolve() (the dependent
+// work), so a thread keeps all its loads in flight at once.
+// (a) the current edge array: fetch the word, resolve its endpoints'
+//     supervertices (two gathers from the L2-resident label array)
 struct SrcEdges {
+    typedef uint64_t Raw;
     const uint64_t *e;
     const int32_t *label;
     Pack pk;
     uint32_t V0;
-    __device__ bool load(int64_t i, uint64_t &k, int32_t &su, int32_t &sv, uint32_t &w) const
+    __device__ __forceinline__ void fetch(int64_t i, Raw &r) const { r = __ldcs(e + i); }
+    __device__ __forceinline__ bool resolve(const Raw &r, uint64_t &k, int32_t &su, int32_t &sv,
+                                            uint32_t &w) const
     {
-        k = e[i];
-        if (pk.a(k) >= V0 || pk.b(k) >= V0) return false;   // never produced for valid input
+        k = r;
+        if (pk.a(k) >= V0 || pk.b(k) >= V0) return false;   // dead words (never real edges)
         su = label[pk.src(k)];
         sv = label[pk.dst(k)];
         w = pk.w(k);
@@ -129,55 +136,54 @@ struct SrcEdges {
     }
 };
 
-// (b) a symmetric CSR (one directed edge per entry); rowid maps entry -> row
-template <typename WT>
-struct SrcCSR {
-    const int32_t *rowid;
-    const int32_t *dest;
-    const WT *weight;
-    int32_t V;
-    Pack pk;
-    int *err;
-    __device__ bool load(int64_t i, uint64_t &k, int32_t &su, int32_t &sv, uint32_t &w) const
-    {
-        int32_t u = rowid[i];
-        if (u < 0) return false;
-        int32_t v = dest[i];
-        if (v < 0 || v >= V) { set_err(err, DEV_BAD_INPUT); return false; }
-        if (u == v) return false;
-        w = wword(weight[i]);
-        k = pk.make(w, (uint32_t)u, (uint32_t)v);
-        su = u;
-        sv = v;
-        return true;
-    }
-};
-
-// (c) both directions of undirected keys (MST selection keys) below a weight cap
+// (b) both directions of undirected keys (MST selection keys) below a weight cap
 struct SrcForest {
+    typedef uint64_t Raw;
     const uint64_t *keys;   // selection keys (w, a, b)
     int64_t n_keys;
     int64_t wmax;           // keep weights <= wmax (-1 keeps none)
     Pack pk;
-    __device__ bool load(int64_t i, uint64_t &k, int32_t &su, int32_t &sv, uint32_t &w) const
+    __device__ __forceinline__ void fetch(int64_t i, Raw &r) const
     {
-        int64_t j = i < n_keys ? i : i - n_keys;
-        uint64_t s = keys[j];
+        r = keys[i < n_keys ? i : i - n_keys];
+    }
+    // resolve() needs the item index for the direction: passed through k
+    __device__ __forceinline__ bool resolve_dir(const Raw &s, bool reverse, uint64_t &k,
+                                                int32_t &su, int32_t &sv, uint32_t &w) const
+    {
         w = pk.sel_w(s);
         if ((int64_t)w > wmax) return false;
-        uint32_t a = pk.sel_a(s), b = pk.sel_b(s);
-        k = (s << 1) | (uint64_t)(i >= n_keys);
-        su = (int32_t)(i < n_keys ? a : b);
-        sv = (int32_t)(i < n_keys ? b : a);
+        const uint32_t a = pk.sel_a(s), b = pk.sel_b(s);
+        k = (s << 1) | (uint64_t)reverse;
+        su = (int32_t)(reverse ? b : a);
+        sv = (int32_t)(reverse ? a : b);
         return true;
     }
 };
 
+template <typename Src>
+__device__ __forceinline__ bool resolve_item(const Src &src, const typename Src::Raw &r,
+                                             int64_t i, uint64_t &k, int32_t &su, int32_t &sv,
+                                             uint32_t &w)
+{
+    return src.resolve(r, k, su, sv, w);
+}
+
+template <>
+__device__ __forceinline__ bool resolve_item<SrcForest>(const SrcForest &src, const uint64_t &r,
+                                                        int64_t i, uint64_t &k, int32_t &su,
+                                                        int32_t &sv, uint32_t &w)
+{
+    return src.resolve_dir(r, i >= src.n_keys, k, su, sv, w);
+}
+
 // Tile kernel: keep-filter + order-preserving compaction + fused min-edge
-// selection for the next round.
+// selection for the next round.  eout may equal the source array (in-place
+// contraction): a tile writes only after its prefix is known, i.e. after
+// every earlier tile has read its input, and never past its own input end.
 template <int MODE, typename Src>
 __global__ void __launch_bounds__(kET)
-k_edge_tile(Src src, int64_t n_in, uint64_t *__restrict__ eout, unsigned long long *best,
+k_edge_tile(Src src, int64_t n_in, uint64_t *eout, unsigned long long *best,
             uint64_t *status, int *counter, int64_t *d_count, int *err)
 {
     __shared__ int s_tile;
@@ -188,20 +194,32 @@ k_edge_tile(Src src, int64_t n_in, uint64_t *__restrict__ eout, unsigned long lo
     const int64_t tile = s_tile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t base = tile * kETile;
-    uint64_t k[kEI];
-    unsigned bal[kEI];
+    typename Src::Raw raw[kEI];
 #pragma unroll
     for (int it = 0; it < kEI; ++it) {
         const int64_t i = base + (int64_t)it * kET + threadIdx.x;
-        int32_t su = 0, sv = 0;
-        uint32_t w = 0;
-        bool keep = false;
+        if (i < n_in) src.fetch(i, raw[it]);
+    }
+    uint64_t k[kEI];
+    int32_t su[kEI], sv[kEI];
+    uint32_t w[kEI];
+    bool keep[kEI];
+#pragma unroll
+    for (int it = 0; it < kEI; ++it) {
+        const int64_t i = base + (int64_t)it * kET + threadIdx.x;
+        su[it] = sv[it] = 0;
+        w[it] = 0;
         k[it] = 0;
-        if (i < n_in) keep = src.load(i, k[it], su, sv, w);
-        bal[it] = __ballot_sync(0xffffffffu, keep);
+        keep[it] = (i < n_in) && resolve_item(src, raw[it], i, k[it], su[it], sv[it], w[it]);
+    }
+    unsigned bal[kEI];
+#pragma unroll
+    for (int it = 0; it < kEI; ++it) {
+        bal[it] = __ballot_sync(0xffffffffu, keep[it]);
         if (lane == 0) s_off[it][warp] = __popc(bal[it]);
-        uint64_t sel = MODE == SEL_MST ? (k[it] >> 1) : (((uint64_t)w << 32) | (uint32_t)sv);
-        seg_min_atomic(keep, su, sel, best);
+        const uint64_t sel =
+            MODE == SEL_MST ? (k[it] >> 1) : (((uint64_t)w[it] << 32) | (uint32_t)sv[it]);
+        seg_min_atomic(keep[it], su[it], sel, best);
     }
     __syncthreads();
     if (warp == 0) {
@@ -248,19 +266,43 @@ k_edge_tile(Src src, int64_t n_in, uint64_t *__restrict__ eout, unsigned long lo
     }
 }
 
-// rowid[e] = v for every entry e of row v (entries outside every row stay -1)
-__global__ void k_rowid(const int32_t *first, const int32_t *deg, int32_t V, int64_t E,
-                        int32_t *rowid, int *err)
+// Round-0 edges straight from a symmetric CSR, one warp per row: entry e
+// becomes edge word e (a self loop or an entry outside every row stays a dead
+// word, dropped by the first contraction); the row's minimum selection key is
+// one atomicMin.
+template <int MODE, typename WT>
+__global__ void k_edges_csr(const int32_t *first, const int32_t *deg, const int32_t *dest,
+                            const WT *weight, int32_t V, int64_t E, Pack pk, uint64_t *eout,
+                            unsigned long long *best, int *err)
 {
     const int lane = threadIdx.x & 31;
-    for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V;
-         v += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        int64_t f = first[v], d = deg[v];
+    for (int64_t u = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < V;
+         u += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int64_t f = first[u], d = deg[u];
         if (f < 0 || d < 0 || f + d > E) {
             if (lane == 0) set_err(err, DEV_BAD_INPUT);
             continue;
         }
-        for (int64_t e = f + lane; e < f + d; e += 32) rowid[e] = (int32_t)v;
+        uint64_t m = kNone;
+        for (int64_t e = f + lane; e < f + d; e += 32) {
+            const int32_t v = dest[e];
+            if (v < 0 || v >= V) {
+                set_err(err, DEV_BAD_INPUT);
+                continue;
+            }
+            if (v == (int32_t)u) continue;          // self loop: stays dead
+            const uint32_t w = wword(weight[e]);
+            const uint64_t k = pk.make(w, (uint32_t)u, (uint32_t)v);
+            eout[e] = k;
+            const uint64_t sel = MODE == SEL_MST ? (k >> 1) : (((uint64_t)w << 32) | (uint32_t)v);
+            m = sel < m ? sel : m;
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
+            m = x < m ? x : m;
+        }
+        if (lane == 0 && m != kNone) atomicMin(&best[u], (unsigned long long)m);
     }
 }
 
@@ -304,6 +346,197 @@ __global__ void k_edges_upper(const int64_t *indptr, const int32_t *indices, con
         }
         if (lane == 0 && m != kNone) atomicMin(&best[i], (unsigned long long)m);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Weight phases (MST mode).  For a strict total order of the edges, the
+// minimum spanning forest of the edges up to a key is exactly the MST
+// restricted to those edges (Kruskal's prefix property).  So the forest is
+// grown phase by phase over weight ranges: a phase contracts the edges of its
+// range whose endpoints are still in different components, then the next
+// phase starts from those components.  Heavy edges that the light ones made
+// internal are dropped by one filtering read instead of being carried through
+// every round.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t wbucket(uint32_t w, int wbits)
+{
+    return wbits <= 8 ? w : (w >> (wbits - 8));
+}
+
+template <typename WT>
+__global__ void k_whist_csr(const WT *weight, int64_t E, int wbits, unsigned long long *hist)
+{
+    __shared__ unsigned long long h[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E;
+         e += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&h[wbucket(wword(weight[e]), wbits) & 255], 1ull);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+__global__ void k_whist_u8(const uint8_t *w, int64_t n, unsigned long long *hist)
+{
+    __shared__ unsigned long long h[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+         e += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&h[w[e]], 1ull);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+// Edges of a symmetric CSR whose weight bucket is in (lo, hi] and whose
+// endpoints are in different components; one warp per row, each 32-entry
+// chunk reserves its output slots with one atomicAdd (edge order is not
+// deterministic, results are: selection uses a strict total order).
+template <typename WT>
+__global__ void k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest,
+                            const WT *weight, int32_t V, int64_t E, int wbits, int lo, int hi,
+                            const int32_t *label, Pack pk, uint64_t *eout,
+                            unsigned long long *cursor, unsigned long long *best, int *err)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int64_t u = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < V;
+         u += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int64_t f = first[u], d = deg[u];
+        if (f < 0 || d < 0 || f + d > E) {
+            if (lane == 0) set_err(err, DEV_BAD_INPUT);
+            continue;
+        }
+        const int32_t lu = label[u];
+        uint64_t m = kNone;
+        for (int64_t e0 = f; e0 < f + d; e0 += 32) {
+            const int64_t e = e0 + lane;
+            bool keep = false;
+            uint64_t k = 0;
+            if (e < f + d) {
+                const int32_t v = dest[e];
+                if (v < 0 || v >= V) {
+                    set_err(err, DEV_BAD_INPUT);
+                } else if (v != (int32_t)u) {
+                    const uint32_t w = wword(weight[e]);
+                    const int b = (int)wbucket(w, wbits);
+                    if (b > lo && b <= hi && label[v] != lu) {
+                        keep = true;
+                        k = pk.make(w, (uint32_t)u, (uint32_t)v);
+                    }
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            if (!bal) continue;
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(cursor, (unsigned long long)__popc(bal));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (keep) {
+                eout[base + __popc(bal & lt)] = k;
+                m = (k >> 1) < m ? (k >> 1) : m;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
+            m = x < m ? x : m;
+        }
+        if (lane == 0 && m != kNone) atomicMin(&best[lu], (unsigned long long)m);
+    }
+}
+
+// Same for an upper-triangle CSR with uint8 weights: both directions of each
+// kept entry.
+__global__ void k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w,
+                              int32_t n, int64_t nnz, int lo, int hi, const int32_t *label,
+                              Pack pk, uint64_t *eout, unsigned long long *cursor,
+                              unsigned long long *best, int *err)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
+         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int64_t s = indptr[i], e_end = indptr[i + 1];
+        if (s < 0 || e_end < s || e_end > nnz) {
+            if (lane == 0) set_err(err, DEV_BAD_INPUT);
+            continue;
+        }
+        const int32_t li = label[i];
+        uint64_t m = kNone;
+        for (int64_t e0 = s; e0 < e_end; e0 += 32) {
+            const int64_t e = e0 + lane;
+            bool keep = false;
+            uint64_t k = 0;
+            int32_t lj = 0;
+            if (e < e_end) {
+                const int32_t j = indices[e];
+                if (j <= i || j >= n) {
+                    set_err(err, DEV_BAD_INPUT);
+                } else {
+                    const uint32_t ww = w[e];
+                    if ((int)ww > lo && (int)ww <= hi) {
+                        lj = label[j];
+                        if (lj != li) {
+                            keep = true;
+                            k = pk.make(ww, (uint32_t)i, (uint32_t)j);
+                        }
+                    }
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            if (!bal) continue;
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(cursor, 2ull * __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (keep) {
+                const unsigned long long at = base + 2ull * __popc(bal & lt);
+                eout[at] = k;            // i -> j
+                eout[at + 1] = k | 1ull; // j -> i
+                m = (k >> 1) < m ? (k >> 1) : m;
+                atomicMin(&best[lj], (unsigned long long)(k >> 1));
+            }
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
+            m = x < m ? x : m;
+        }
+        if (lane == 0 && m != kNone) atomicMin(&best[li], (unsigned long long)m);
+    }
+}
+
+// Phase ranges (lo, hi] of weight buckets: cut the bucket histogram at the
+// given cumulative fractions of the entries.
+static int phase_ranges(const unsigned long long *hist, const double *fracs, int nf, int *lo,
+                        int *hi)
+{
+    unsigned long long tot = 0;
+    for (int b = 0; b < 256; ++b) tot += hist[b];
+    int np = 0, prev = -1;
+    unsigned long long acc = 0;
+    int b = 0;
+    for (int f = 0; f < nf; ++f) {
+        const double target = fracs[f] * (double)tot;
+        while (b < 255 && (double)(acc + hist[b]) < target) acc += hist[b++];
+        const int cut = (f == nf - 1) ? 255 : b;
+        if (cut > prev) {
+            lo[np] = prev;
+            hi[np] = cut;
+            np++;
+            prev = cut;
+        }
+        if (cut == 255) break;
+        acc += hist[b];
+        b++;
+    }
+    if (prev < 255) {
+        lo[np] = prev;
+        hi[np] = 255;
+        np++;
+    }
+    return np;
 }
 
 __global__ void k_iota(int32_t *a, int64_t n)
@@ -426,15 +659,17 @@ __global__ void k_key2eid(const uint64_t *keys, int64_t n_keys, const int32_t *f
 // ---------------------------------------------------------------------------
 struct Engine {
     int *err;
-    int64_t *cnt;             // [0] edges out, [1] vertices out, [2] emitted
+    int64_t *cnt;             // [0] edges out, [1] vertices out, [2] emitted, [3] phase cursor
     uint64_t *ea, *eb;
     int32_t *label;
     unsigned long long *best;
     int32_t *succ, *color, *flag, *pos;
     uint64_t *mst;
+    unsigned long long *hist; // 256 weight buckets
     ScanScratch scan;
     int32_t V0;
     int64_t Emax;
+    int64_t mst_base = 0;     // forest edges emitted by earlier phases
     int max_rounds = 96;      // lowered only by the round-trace debug entry point
 
     static Engine carve(Carver &c, int32_t V0, int64_t Emax)
@@ -442,10 +677,13 @@ struct Engine {
         Engine g;
         g.err = c.take<int>(1);
         g.cnt = c.take<int64_t>(4);
+        g.hist = c.take<unsigned long long>(256);
         g.V0 = V0;
         g.Emax = Emax;
+        // one edge array (contraction is in place); eb holds the two
+        // directions of a forest (at most 2 V0 words) for the final clustering
         g.ea = c.take<uint64_t>(Emax > 0 ? Emax : 1);
-        g.eb = c.take<uint64_t>(Emax > 0 ? Emax : 1);
+        g.eb = c.take<uint64_t>(2 * (size_t)V0);
         g.label = c.take<int32_t>(V0);
         g.best = c.take<unsigned long long>(V0);
         g.succ = c.take<int32_t>(V0);
@@ -464,6 +702,43 @@ struct Engine {
         EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
         EACB_CUDA(cudaStreamSynchronize(st));
         return dev_err_to_status(e);
+    }
+
+    // MST by weight phases (see k_phase_csr).  `hist` must hold the 256-bucket
+    // weight histogram; build(lo, hi) launches one phase's edge build into ea
+    // (slots reserved through cnt[3]) with its selection into best.
+    template <typename Build>
+    int run_phased(Pack pk, Build build, cudaStream_t st, int64_t *n_mst_out, int64_t *n_comp_out)
+    {
+        unsigned long long h[256];
+        EACB_CUDA(cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, st));
+        EACB_CUDA(cudaStreamSynchronize(st));
+        const double fracs[3] = {0.125, 0.5, 1.0};
+        int lo[8], hi[8];
+        const int np = phase_ranges(h, fracs, 3, lo, hi);
+        int32_t V = V0;
+        mst_base = 0;
+        for (int q = 0; q < np; ++q) {
+            EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V, st));
+            EACB_CUDA(cudaMemsetAsync(&cnt[3], 0, sizeof(int64_t), st));
+            int s = build(lo[q], hi[q]);
+            if (s) return s;
+            int64_t Ep = 0;
+            int e = 0;
+            EACB_CUDA(cudaMemcpyAsync(&Ep, &cnt[3], sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+            EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+            EACB_CUDA(cudaStreamSynchronize(st));
+            if (e) return dev_err_to_status(e);
+            if (Ep > Emax) return EACB_ERR_INTERNAL;
+            int64_t nm = 0, nc = 0;
+            if ((s = run<SEL_MST>(pk, Ep, V, st, &nm, &nc))) return s;
+            mst_base += nm;
+            V = (int32_t)nc;
+            if (V <= 1) break;
+        }
+        *n_mst_out = mst_base;
+        *n_comp_out = V;
+        return EACB_OK;
     }
 
     int reset(cudaStream_t st)
@@ -496,12 +771,18 @@ struct Engine {
     // their selection.  On return: label = component of every vertex,
     // *n_comp = number of components, *n_mst = emitted forest edges.
     template <int MODE>
-    int run(Pack pk, int64_t E0, cudaStream_t st, int64_t *n_mst_out, int64_t *n_comp_out)
+    int run(Pack pk, int64_t E0, int32_t V_start, cudaStream_t st, int64_t *n_mst_out,
+            int64_t *n_comp_out)
     {
-        int32_t V = V0;
+        int32_t V = V_start;
         int64_t E = E0;
         int64_t n_mst = 0;
-        uint64_t *ein = ea, *eout = eb;
+        if (E0 == 0) {                 // nothing to contract: components stay as they are
+            *n_mst_out = 0;
+            *n_comp_out = V_start;
+            return EACB_OK;
+        }
+        uint64_t *ein = ea, *eout = ea;          // in-place contraction
         for (int round = 0; round < max_rounds; ++round) {
             const unsigned gv = grid_for(V, 256);
             k_select<MODE><<<gv, 256, 0, st>>>(best, succ, V, label, pk);
@@ -511,7 +792,7 @@ struct Engine {
             if (MODE == SEL_MST) {
                 int s = scan_launch<int32_t, int32_t>(flag, pos, V, 0, &cnt[2], scan, st);
                 if (s) return s;
-                k_emit<<<gv, 256, 0, st>>>(best, flag, pos, mst + n_mst, V);
+                k_emit<<<gv, 256, 0, st>>>(best, flag, pos, mst + mst_base + n_mst, V);
                 EACB_CHECK_LAUNCH();
             }
             k_jump<<<gv, 256, 0, st>>>(color, V, err);
@@ -551,9 +832,6 @@ struct Engine {
             if (MODE == SEL_MST) n_mst += h[2];
             int32_t Vn = (int32_t)h[1];
             int64_t En = h[0];
-            uint64_t *t = ein;
-            ein = eout;
-            eout = t;
             if (Vn <= 1 || En == 0) {
                 *n_mst_out = n_mst;
                 *n_comp_out = Vn;
@@ -585,25 +863,45 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
     if (s) return s;
     Carver c(ws, ws_bytes);
     Engine g = Engine::carve(c, V, E);
-    int32_t *rowid = c.take<int32_t>(E > 0 ? E : 1);
     if (c.overflow) return EACB_ERR_WORKSPACE;
     if ((s = g.reset(st))) return s;
-    if (E > 0) {
-        EACB_CUDA(cudaMemsetAsync(rowid, 0xff, sizeof(int32_t) * E, st));
-        k_rowid<<<grid_for((int64_t)V * 32, 256), 256, 0, st>>>(first, deg, V, E, rowid, g.err);
-        EACB_CHECK_LAUNCH();
-    }
-    SrcCSR<WT> src{rowid, dest, weight, V, pk, g.err};
     int64_t h[3];
-    if (mode == SEL_MST) s = g.filter<SEL_MST>(src, E, g.ea, st);
-    else s = g.filter<SEL_CC>(src, E, g.ea, st);
-    if (s) return s;
-    if ((s = g.read_counts(st, h))) return s;
     int64_t n_mst = 0, n_comp = 0;
     if (g_debug_rounds > 0) g.max_rounds = g_debug_rounds;
-    if (mode == SEL_MST) s = g.run<SEL_MST>(pk, h[0], st, &n_mst, &n_comp);
-    else s = g.run<SEL_CC>(pk, h[0], st, &n_mst, &n_comp);
-    if (s) return s;
+    const unsigned gr = grid_for((int64_t)V * 32, 256);
+    if (mode == SEL_MST && g_debug_rounds == 0) {
+        // weight phases over the bucket histogram of the entries
+        EACB_CUDA(cudaMemsetAsync(g.hist, 0, 256 * sizeof(unsigned long long), st));
+        if (E > 0) {
+            k_whist_csr<WT><<<grid_for(E, 256, 148 * 8), 256, 0, st>>>(weight, E, wbits, g.hist);
+            EACB_CHECK_LAUNCH();
+        }
+        auto build = [&](int lo, int hi) -> int {
+            if (E == 0) return EACB_OK;
+            k_phase_csr<WT><<<gr, 256, 0, st>>>(first, deg, dest, weight, V, E, wbits, lo, hi,
+                                                g.label, pk, g.ea,
+                                                (unsigned long long *)&g.cnt[3], g.best, g.err);
+            EACB_CHECK_LAUNCH();
+            return EACB_OK;
+        };
+        if ((s = g.run_phased(pk, build, st, &n_mst, &n_comp))) return s;
+    } else {
+        if (E > 0) {
+            // dead words everywhere first: entries outside every row, self loops
+            EACB_CUDA(cudaMemsetAsync(g.ea, 0xff, sizeof(uint64_t) * E, st));
+            if (mode == SEL_MST)
+                k_edges_csr<SEL_MST, WT><<<gr, 256, 0, st>>>(first, deg, dest, weight, V, E, pk,
+                                                             g.ea, g.best, g.err);
+            else
+                k_edges_csr<SEL_CC, WT><<<gr, 256, 0, st>>>(first, deg, dest, weight, V, E, pk,
+                                                            g.ea, g.best, g.err);
+            EACB_CHECK_LAUNCH();
+        }
+        if ((s = g.read_counts(st, h))) return s;      // input validity before the rounds
+        if (mode == SEL_MST) s = g.run<SEL_MST>(pk, E, V, st, &n_mst, &n_comp);
+        else s = g.run<SEL_CC>(pk, E, V, st, &n_mst, &n_comp);
+        if (s) return s;
+    }
     if (mode == SEL_MST) {
         if (n_mst > 0) {
             k_key2eid<WT><<<grid_for(n_mst * 32, 256), 256, 0, st>>>(g.mst, n_mst, first, deg, dest,
@@ -772,7 +1070,6 @@ extern "C" size_t eacb_boruvka_workspace_size(int32_t n_vertices, int64_t n_edge
 {
     Carver c(nullptr, 0);
     Engine::carve(c, n_vertices, n_edges);
-    c.take<int32_t>(n_edges > 0 ? n_edges : 1);
     return c.off;
 }
 
@@ -841,16 +1138,22 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
     carve_final(c, n, nnz, &g, &hist, &plan, &cmin);
     if (c.overflow) return EACB_ERR_WORKSPACE;
     if ((s = g.reset(st))) return s;
-    // 1. minimum spanning forest of the dissimilarity graph
+    // 1. minimum spanning forest of the dissimilarity graph, by weight phases
+    EACB_CUDA(cudaMemsetAsync(g.hist, 0, 256 * sizeof(unsigned long long), st));
     if (nnz > 0) {
-        k_edges_upper<SEL_MST><<<grid_for((int64_t)n * 32, 256), 256, 0, st>>>(
-            indptr, indices, diassoc, n, nnz, pk, g.ea, g.best, g.err);
+        k_whist_u8<<<grid_for(nnz, 256, 148 * 8), 256, 0, st>>>(diassoc, nnz, g.hist);
         EACB_CHECK_LAUNCH();
     }
-    int64_t h0[3];
-    if ((s = g.read_counts(st, h0))) return s;     // input validity before the rounds
     int64_t n_mst = 0, n_comp = 0;
-    if ((s = g.run<SEL_MST>(pk, 2 * nnz, st, &n_mst, &n_comp))) return s;
+    auto build = [&](int lo, int hi) -> int {
+        if (nnz == 0) return EACB_OK;
+        k_phase_upper<<<grid_for((int64_t)n * 32, 256), 256, 0, st>>>(
+            indptr, indices, diassoc, n, nnz, lo, hi, g.label, pk, g.ea,
+            (unsigned long long *)&g.cnt[3], g.best, g.err);
+        EACB_CHECK_LAUNCH();
+        return EACB_OK;
+    };
+    if ((s = g.run_phased(pk, build, st, &n_mst, &n_comp))) return s;
     // 2. lifetime rule on the weight histogram
     EACB_CUDA(cudaMemsetAsync(hist, 0, 256 * sizeof(int64_t), st));
     if (n_mst > 0) {
@@ -881,7 +1184,7 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
     // run() starts from ea: swap roles by copying (forest is small)
     EACB_CUDA(cudaMemcpyAsync(g.ea, g.eb, sizeof(uint64_t) * h[0], cudaMemcpyDeviceToDevice, st));
     int64_t nm2 = 0, nc2 = 0;
-    if ((s = g.run<SEL_CC>(pk, h[0], st, &nm2, &nc2))) return s;
+    if ((s = g.run<SEL_CC>(pk, h[0], n, st, &nm2, &nc2))) return s;
     // 4. number components by their smallest member
     EACB_CUDA(cudaMemsetAsync(cmin, 0x7f, sizeof(int32_t) * n, st));
     const unsigned gn = grid_for(n, 256);

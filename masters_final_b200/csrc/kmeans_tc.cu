@@ -2,20 +2,20 @@
 //
 // dist(x, c) = |x|^2 - 2 x.c + |c|^2 on data centred at its mean.  The dot
 // products run as ONE BF16 GEMM with FP32 accumulation in tensor memory:
-// each float32 operand is split into a BF16 high part and a BF16 low part
-// (x = xh + xl + O(2^-16 |x|)), and the K dimension concatenates
-// [xh, xh, xl] . [ch, cl, ch] so the product carries ~16 significant bits.
-// The epilogue (8 warps, one point row per thread, half the columns per
-// warp pair) reads the accumulator tile from TMEM with tcgen05.ld, forms the
-// screened distance and keeps the best two per point.  A point whose
-// runner-up lies within the error bound 2 E (|x|^2 + max|c|^2) of its winner
-// (E derived from the BF16 split and the FP32 accumulation, times 2) is
-// re-labelled by the reference's exact loop; every other point gets its
-// winner's exact reference distance.  Labels therefore equal the
-// reference's (MyML/MyML/cluster/KMeans.py:453-490) for any input.
+// each float32 operand is split into three BF16 parts (h + m + l, ~24
+// significant bits) and the K dimension holds the six products that matter
+// (see put_row), the large h*h group last.  The epilogue (8 warps, one point
+// row per thread, half the columns per warp pair) reads the accumulator tile
+// from TMEM with tcgen05.ld, forms the screened distance and keeps the best
+// two per point.  A point whose runner-up lies within the proven error bound
+// E (|x|^2 + max|c|^2) of its winner (E from the split, the accumulation
+// order and the epilogue arithmetic, times 2) is re-labelled by the
+// reference's exact loop; every other point gets its winner's exact
+// reference distance.  Labels therefore equal the reference's
+// (MyML/MyML/cluster/KMeans.py:453-490) for any input.
 //
-// Shapes: M = 128 points per CTA, N <= 256 centroids per MMA tile, K = 3d
-// padded to a multiple of 16 (<= 96).  Operands are pre-arranged in global
+// Shapes: M = 128 points per CTA, N <= 256 centroids per MMA tile, K = 6d
+// padded to a multiple of 16 (<= 192).  Operands are pre-arranged in global
 // memory in the UMMA K-major no-swizzle core-matrix layout (8 rows x 16
 // bytes per core matrix, LBO = 128 B along K, SBO = 128 B * K/8 along M/N),
 // so each tile is one contiguous cp.async.bulk copy into shared memory.
@@ -170,22 +170,33 @@ __global__ void k_mean(const double *part, int nblocks, int32_t n, int32_t D, fl
     mu[d] = (float)(t / (double)n);
 }
 
-// rows of one operand: centred, split into BF16 hi/lo, placed in the blocked
-// layout; `order` selects [hi,hi,lo] (points) or [hi,lo,hi] (centroids).
+// Rows of one operand, centred and split into three BF16 parts
+// v = h + m + l (each part the BF16 rounding of the remainder, so |m| <=
+// 2^-8 |v|, |l| <= 2^-16 |v| and the rest is below 2^-24 |v|).  The K axis
+// holds six groups of D products, smallest first so that the large h*h
+// products are accumulated last:
+//   group      0    1    2    3    4    5
+//   point      l    m    h    m    h    h
+//   centroid   h    m    l    h    m    h
+// Their sum is x.c up to the dropped l*m, m*l, l*l terms (< 3 * 2^-24 |x||c|).
 __device__ __forceinline__ void put_row(const float *v, const float *mu, int D, int Kp, int row,
                                        uint8_t *tile, bool point_side, float &norm)
 {
+    constexpr int kPointPart[6] = {2, 1, 0, 1, 0, 0};      // 0 = h, 1 = m, 2 = l
+    constexpr int kCentPart[6] = {0, 1, 2, 0, 1, 0};
     float nrm = 0.f;
     for (int k = 0; k < Kp; ++k) {
         __nv_bfloat16 b = __float2bfloat16_rn(0.f);
-        if (k < 3 * D) {
-            const int d = k % D, part = k / D;
+        if (k < 6 * D) {
+            const int d = k % D, grp = k / D;
             const float xc = __fsub_rn(v[d], mu[d]);
-            const __nv_bfloat16 hi = __float2bfloat16_rn(xc);
-            const __nv_bfloat16 lo = __float2bfloat16_rn(__fsub_rn(xc, __bfloat162float(hi)));
-            const bool use_lo = point_side ? (part == 2) : (part == 1);
-            b = use_lo ? lo : hi;
-            if (part == 0) nrm = fmaf(xc, xc, nrm);
+            const __nv_bfloat16 h = __float2bfloat16_rn(xc);
+            const float r1 = __fsub_rn(xc, __bfloat162float(h));
+            const __nv_bfloat16 m = __float2bfloat16_rn(r1);
+            const __nv_bfloat16 l = __float2bfloat16_rn(__fsub_rn(r1, __bfloat162float(m)));
+            const int part = point_side ? kPointPart[grp] : kCentPart[grp];
+            b = part == 0 ? h : (part == 1 ? m : l);
+            if (grp == 0) nrm = fmaf(xc, xc, nrm);
         }
         *reinterpret_cast<__nv_bfloat16 *>(tile + core_off(row, k, Kp)) = b;
     }
@@ -235,7 +246,7 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
            const int32_t *__restrict__ kk, int32_t kmax, int32_t kt_max,
            const int32_t *__restrict__ active, const uint8_t *__restrict__ A,
            const float *__restrict__ nx, const uint8_t *__restrict__ B,
-           const float *__restrict__ nc, const float *__restrict__ cmax2, float E,
+           const float *__restrict__ nc, const float *__restrict__ cmax2, float E, int nbuf,
            int32_t *labels, float *dists, int32_t *amb, int *namb, int *err)
 {
     extern __shared__ __align__(1024) uint8_t smem[];
@@ -250,7 +261,9 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
     const int tiles = (K + kTN - 1) / kTN;
     const uint32_t a_bytes = (uint32_t)kTM * Kp * 2, b_bytes = (uint32_t)kTN * Kp * 2;
     uint8_t *sA = smem;
-    uint8_t *sB[2] = {smem + a_bytes, smem + a_bytes + b_bytes};
+    // two centroid-tile buffers when they fit (prefetch overlaps the MMA),
+    // else one (prefetch overlaps the epilogue)
+    uint8_t *sB[2] = {smem + a_bytes, nbuf == 2 ? smem + a_bytes + b_bytes : smem + a_bytes};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t tile0 = blockIdx.x;
     const uint8_t *Ap = A + tile0 * a_bytes;
@@ -292,7 +305,7 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
     uint32_t ph_b[2] = {0, 0}, ph_mma = 0;
     bool ok = true;
     for (int t = 0; t < tiles && ok; ++t) {
-        const int buf = t & 1;
+        const int buf = nbuf == 2 ? (t & 1) : 0;
         const int nvalid = min(kTN, K - t * kTN);
         const int N = (nvalid + 15) & ~15;
         if (threadIdx.x == 0) {
@@ -309,7 +322,7 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
                     mma_bf16(tmem, ad, bd, idesc, s > 0 ? 1u : 0u);
                 }
                 mma_commit(&bar_mma);
-                if (t + 1 < tiles) {
+                if (nbuf == 2 && t + 1 < tiles) {
                     // the other buffer's last reader (MMA of tile t-1) completed
                     mbar_expect_tx(&bar_b[buf ^ 1], b_bytes);
                     bulk_g2s(sB[buf ^ 1], Bp + (int64_t)(t + 1) * b_bytes, b_bytes, &bar_b[buf ^ 1]);
@@ -322,6 +335,10 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
         if (!mbar_wait(&bar_mma, ph_mma)) {
             set_err(err, DEV_SPIN_LIMIT);
             s_fail = 1;
+        } else if (nbuf == 1 && threadIdx.x == 0 && t + 1 < tiles) {
+            // single buffer: this tile's MMA has finished reading it
+            mbar_expect_tx(&bar_b[0], b_bytes);
+            bulk_g2s(sB[0], Bp + (int64_t)(t + 1) * b_bytes, b_bytes, &bar_b[0]);
         }
         ph_mma ^= 1;
         tc_fence_after();
@@ -360,9 +377,12 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
         int wi;
         if (o1 < b1) { w1 = o1; wi = oi; w2 = fminf(b1, o2); }
         else { w1 = b1; wi = i1; w2 = fminf(o1, b2); }
-        const float bound = 2.f * E * (xn + cmax2[p]);
+        // each screened distance is within E/2 (|x|^2 + max|c|^2) of the
+        // exact one (E carries a factor 2 of margin): the winner is certain
+        // when the runner-up is more than twice that above it
+        const float bound = E * (xn + cmax2[p]);
         const int64_t o = (int64_t)p * n + i;
-        if (w2 - w1 > 2.f * bound) {
+        if (w2 - w1 > bound) {
             float xv[32];
             for (int d = 0; d < D; ++d) xv[d] = X[i * D + d];
             labels[o] = wi;
@@ -441,7 +461,7 @@ size_t tc_scratch_bytes(int32_t n, int32_t D, int32_t P, int32_t kmax)
 TcScratch TcScratch::carve(Carver &c, int32_t n, int32_t D, int32_t P, int32_t kmax)
 {
     TcScratch s;
-    s.Kp = ((3 * D + 15) / 16) * 16;
+    s.Kp = ((6 * D + 15) / 16) * 16;
     s.n_pad = ((int64_t)n + kTM - 1) / kTM * kTM;
     s.kt_max = (kmax + kTN - 1) / kTN;
     s.A = c.take<uint8_t>((size_t)s.n_pad * s.Kp * 2);
@@ -478,9 +498,20 @@ int label_pass_tc(const float *X, int32_t n, int32_t D, int32_t P, const float *
     // error model of the screened distance, doubled for margin: BF16 split
     // (3 * 2^-16), FP32 accumulation over 3D products (3D * 2^-23), the
     // norms and the epilogue arithmetic ((D + 6) * 2^-24)
-    const float E = 2.f * (float)(3.0 * ldexp(1.0, -16) + 3.0 * D * ldexp(1.0, -23) +
-                                  (D + 6) * ldexp(1.0, -24));
-    const size_t smem = (size_t)kTM * s.Kp * 2 + 2 * (size_t)kTN * s.Kp * 2;
+    // Error model of the screened distance, doubled for margin.  The dot
+    // product: the three-way split drops < 3 * 2^-24 |x||c|; the MMA adds
+    // the h*h group last, so its accumulation error is at most
+    // (16 ceil(D/16) + 3) 2^-23 of sum|x_d c_d| (<= |x||c|), the earlier,
+    // 2^8-times smaller groups add less than one more 2^-23.  Norms and the
+    // epilogue: (D + 6) 2^-24 of |x|^2 + |c|^2.  With 2|x||c| <= |x|^2 +
+    // |c|^2 the screened distance is within E (|x|^2 + max|c|^2) / 2.
+    const double dot_err = 3.0 * ldexp(1.0, -24) +
+                           (16.0 * ((D + 15) / 16) + 4.0) * ldexp(1.0, -23);
+    const float E = 2.f * (float)(dot_err + (D + 6) * ldexp(1.0, -24));
+    const size_t a_bytes = (size_t)kTM * s.Kp * 2, b_bytes = (size_t)kTN * s.Kp * 2;
+    // double-buffer the centroid tiles only while two CTAs still fit per SM
+    const int nbuf = (a_bytes + 2 * b_bytes <= 110 * 1024) ? 2 : 1;
+    const size_t smem = a_bytes + nbuf * b_bytes;
     // at least 100 KB so that no more than two CTAs (2 x 256 TMEM columns)
     // share an SM
     const size_t smem_req = smem < 100 * 1024 ? 100 * 1024 : smem;
@@ -489,7 +520,7 @@ int label_pass_tc(const float *X, int32_t n, int32_t D, int32_t P, const float *
     dim3 grid((unsigned)(s.n_pad / kTM), (unsigned)P);
     ProfScope ps(PROF_KMEANS, st);
     k_label_tc<<<grid, kTThreads, smem_req, st>>>(X, n, D, s.Kp, C, kk, kmax, s.kt_max, active,
-                                                  s.A, s.nx, s.B, s.nc, s.cmax2, E, labels, dists,
+                                                  s.A, s.nx, s.B, s.nc, s.cmax2, E, nbuf, labels, dists,
                                                   amb, namb, s.err);
     EACB_CHECK_LAUNCH();
     ps.done(0.0);
