@@ -26,6 +26,8 @@
 #include "eacb_common.cuh"
 #include "scan_impl.cuh"
 
+#include <vector>
+
 namespace eacb {
 
 enum { SEL_MST = 0, SEL_CC = 1 };
@@ -184,14 +186,23 @@ __device__ __forceinline__ bool resolve_item<SrcForest>(const SrcForest &src, co
 template <int MODE, typename Src>
 __global__ void __launch_bounds__(kET)
 k_edge_tile(Src src, int64_t n_in, uint64_t *eout, unsigned long long *best,
-            uint64_t *status, int *counter, int64_t *d_count, int *err)
+            uint64_t *status, int *counter, int64_t *d_count, int *err,
+            const int64_t *d_n = nullptr)
 {
     __shared__ int s_tile;
     __shared__ int s_off[kEI][kET / 32];
     __shared__ int64_t s_prefix;
+    // with d_n the edge count is read on the device and the blocks loop over
+    // tiles (persistent grid); tile ids are taken in increasing order, so
+    // every tile a block waits on is held by a running block
+    if (d_n) n_in = *d_n;
+    const int64_t n_tiles = (n_in + kETile - 1) / kETile;
+    for (;;) {
     if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
     __syncthreads();
     const int64_t tile = s_tile;
+    __syncthreads();
+    if (tile >= n_tiles) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t base = tile * kETile;
     typename Src::Raw raw[kEI];
@@ -263,6 +274,9 @@ k_edge_tile(Src src, int64_t n_in, uint64_t *eout, unsigned long long *best,
             int64_t pos = s_prefix + s_off[it][warp] + __popc(bal[it] & lt);
             eout[pos] = k[it];
         }
+    }
+    if (!d_n) return;            // one tile per block
+    __syncthreads();             // shared state is reused by the next tile
     }
 }
 
@@ -546,11 +560,27 @@ __global__ void k_iota(int32_t *a, int64_t n)
         a[i] = (int32_t)i;
 }
 
+// Round state kept on the device, so that a round needs no host value and
+// the rounds can loop inside one CUDA graph (see Engine::run):
+enum : int {
+    C_E_NEXT = 0,     // edges after this round's contraction (filter total)
+    C_V_NEXT = 1,     // supervertices after this round (root-scan total)
+    C_EMIT = 2,       // forest edges emitted this round (emit-scan total)
+    C_CURSOR = 3,     // phase-build output cursor
+    C_V = 4,          // supervertices at the start of the round
+    C_E = 5,          // edges at the start of the round
+    C_NMST = 6,       // forest edges emitted so far (all phases)
+    C_ROUNDS = 7,     // rounds run in this phase
+    C_DONE = 8,       // 1 once the phase has converged
+    C_COUNT = 16
+};
+
 // successor of each supervertex from its selected key
 template <int MODE>
-__global__ void k_select(const unsigned long long *best, int32_t *succ, int32_t V,
+__global__ void k_select(const unsigned long long *best, int32_t *succ, const int64_t *dV,
                          const int32_t *label, Pack pk)
 {
+    const int64_t V = *dV;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
          s += (int64_t)gridDim.x * blockDim.x) {
         uint64_t b = best[s];
@@ -568,8 +598,9 @@ __global__ void k_select(const unsigned long long *best, int32_t *succ, int32_t 
 }
 
 // mutual picks: the smaller id drops its edge (MyML/MyML/graph/mst.py:283-305)
-__global__ void k_mirror(const int32_t *succ, int32_t *color, int32_t *emit, int32_t V)
+__global__ void k_mirror(const int32_t *succ, int32_t *color, int32_t *emit, const int64_t *dV)
 {
+    const int64_t V = *dV;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
          s += (int64_t)gridDim.x * blockDim.x) {
         int32_t t = succ[s];
@@ -580,20 +611,24 @@ __global__ void k_mirror(const int32_t *succ, int32_t *color, int32_t *emit, int
     }
 }
 
+// forest edges of this round, appended after the ones of earlier rounds
 __global__ void k_emit(const unsigned long long *best, const int32_t *emit, const int32_t *pos,
-                       uint64_t *out, int32_t V)
+                       uint64_t *out, const int64_t *dV, const int64_t *d_base)
 {
+    const int64_t V = *dV;
+    uint64_t *o = out + *d_base;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
          s += (int64_t)gridDim.x * blockDim.x)
-        if (emit[s]) out[pos[s]] = best[s];
+        if (emit[s]) o[pos[s]] = best[s];
 }
 
 // roots by pointer chasing with path halving; bounded (a non-forest errors).
 // A halving step replaces c's parent p by its grandparent g only if c still
 // points at p (compare-and-swap): a plain store could overwrite the root that
 // c's own thread already stored, leaving c on a non-root.
-__global__ void k_jump(int32_t *color, int32_t V, int *err)
+__global__ void k_jump(int32_t *color, const int64_t *dV, int *err)
 {
+    const int64_t V = *dV;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
          s += (int64_t)gridDim.x * blockDim.x) {
         int32_t c = color[s];
@@ -613,8 +648,9 @@ __global__ void k_jump(int32_t *color, int32_t V, int *err)
     }
 }
 
-__global__ void k_rootflag(const int32_t *color, int32_t *flag, int32_t V)
+__global__ void k_rootflag(const int32_t *color, int32_t *flag, const int64_t *dV)
 {
+    const int64_t V = *dV;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
          s += (int64_t)gridDim.x * blockDim.x)
         flag[s] = color[s] == (int32_t)s;
@@ -625,6 +661,53 @@ __global__ void k_relabel(int32_t *label, const int32_t *color, const int32_t *n
     for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < V0;
          x += (int64_t)gridDim.x * blockDim.x)
         label[x] = newid[color[label[x]]];
+}
+
+// Clears the next round's selection and the contraction's look-back state.
+__global__ void k_round_reset(unsigned long long *best, const int64_t *dV, uint64_t *status,
+                              int64_t n_status, int *counter, int64_t *d_count)
+{
+    const int64_t V = *dV;
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t s = t0; s < V; s += stride) best[s] = kNone;
+    for (int64_t s = t0; s < n_status; s += stride) status[s] = 0;
+    if (t0 == 0) {
+        *counter = 0;
+        *d_count = 0;
+    }
+}
+
+__global__ void k_round_begin(int64_t *cnt, int64_t V, int64_t E)
+{
+    if (threadIdx.x == 0) {
+        cnt[C_V] = V;
+        cnt[C_E] = E;
+        cnt[C_ROUNDS] = 0;
+        cnt[C_DONE] = 0;
+    }
+}
+
+// End of a round: advance the sizes and decide whether another round runs.
+// cnt[C_DONE]: 0 = continue, 1 = converged (one supervertex or no edge
+// left), 2 = no contraction (an error), 3 = round limit, 4 = device error.
+// Inside a graph, the loop condition is cleared when the phase is done.
+__global__ void k_round_end(int64_t *cnt, int is_mst, int max_rounds, const int *err,
+                            cudaGraphConditionalHandle h, int use_handle)
+{
+    if (threadIdx.x != 0) return;
+    const int64_t V = cnt[C_V], Vn = cnt[C_V_NEXT], En = cnt[C_E_NEXT];
+    if (is_mst) cnt[C_NMST] += cnt[C_EMIT];
+    const int64_t r = ++cnt[C_ROUNDS];
+    int64_t done = 0;
+    if (*(volatile const int *)err) done = 4;
+    else if (Vn <= 1 || En == 0) done = 1;
+    else if (Vn >= V) done = 2;
+    else if (r >= max_rounds) done = 3;
+    cnt[C_DONE] = done;
+    cnt[C_V] = Vn;
+    cnt[C_E] = En;
+    if (use_handle) cudaGraphSetConditional(h, done ? 0u : 1u);
 }
 
 // MST selection key -> index of its entry in row min(u,v) of a symmetric CSR
@@ -659,7 +742,7 @@ __global__ void k_key2eid(const uint64_t *keys, int64_t n_keys, const int32_t *f
 // ---------------------------------------------------------------------------
 struct Engine {
     int *err;
-    int64_t *cnt;             // [0] edges out, [1] vertices out, [2] emitted, [3] phase cursor
+    int64_t *cnt;             // round state, indexed by C_E_NEXT .. C_DONE
     uint64_t *ea, *eb;
     int32_t *label;
     unsigned long long *best;
@@ -676,7 +759,7 @@ struct Engine {
     {
         Engine g;
         g.err = c.take<int>(1);
-        g.cnt = c.take<int64_t>(4);
+        g.cnt = c.take<int64_t>(C_COUNT);
         g.hist = c.take<unsigned long long>(256);
         g.V0 = V0;
         g.Emax = Emax;
@@ -706,7 +789,7 @@ struct Engine {
 
     // MST by weight phases (see k_phase_csr).  `hist` must hold the 256-bucket
     // weight histogram; build(lo, hi) launches one phase's edge build into ea
-    // (slots reserved through cnt[3]) with its selection into best.
+    // (slots reserved through cnt[C_CURSOR]) with its selection into best.
     template <typename Build>
     int run_phased(Pack pk, Build build, cudaStream_t st, int64_t *n_mst_out, int64_t *n_comp_out)
     {
@@ -720,12 +803,13 @@ struct Engine {
         mst_base = 0;
         for (int q = 0; q < np; ++q) {
             EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V, st));
-            EACB_CUDA(cudaMemsetAsync(&cnt[3], 0, sizeof(int64_t), st));
+            EACB_CUDA(cudaMemsetAsync(&cnt[C_CURSOR], 0, sizeof(int64_t), st));
             int s = build(lo[q], hi[q]);
             if (s) return s;
             int64_t Ep = 0;
             int e = 0;
-            EACB_CUDA(cudaMemcpyAsync(&Ep, &cnt[3], sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+            EACB_CUDA(cudaMemcpyAsync(&Ep, &cnt[C_CURSOR], sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                      st));
             EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
             EACB_CUDA(cudaStreamSynchronize(st));
             if (e) return dev_err_to_status(e);
@@ -744,7 +828,7 @@ struct Engine {
     int reset(cudaStream_t st)
     {
         EACB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
-        EACB_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int64_t), st));
+        EACB_CUDA(cudaMemsetAsync(cnt, 0, C_COUNT * sizeof(int64_t), st));
         EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V0, st));
         k_iota<<<grid_for(V0, 256), 256, 0, st>>>(label, V0);
         EACB_CHECK_LAUNCH();
@@ -767,88 +851,236 @@ struct Engine {
         return EACB_OK;
     }
 
+    int edge_grid() const
+    {
+        const int64_t t = (Emax + kETile - 1) / kETile;
+        return (int)(t < 148 * 8 ? (t > 0 ? t : 1) : 148 * 8);
+    }
+
+    // One Boruvka round with every size read on the device (cnt[C_V],
+    // cnt[C_E]); identical launch shapes every round, so the sequence can be
+    // captured once into a CUDA graph.  With use_handle the last kernel sets
+    // the graph's loop condition.  Returns the kernels it launches per round
+    // in *per_round.
+    template <int MODE>
+    int enqueue_round(Pack pk, cudaStream_t st, int use_handle, cudaGraphConditionalHandle h,
+                      bool timed_filter, int *per_round)
+    {
+        const unsigned gv = 296;
+        int launches = 0;
+        k_select<MODE><<<gv, 256, 0, st>>>(best, succ, &cnt[C_V], label, pk);
+        EACB_CHECK_LAUNCH();
+        k_mirror<<<gv, 256, 0, st>>>(succ, color, MODE == SEL_MST ? flag : nullptr, &cnt[C_V]);
+        EACB_CHECK_LAUNCH();
+        launches += 2;
+        if (MODE == SEL_MST) {
+            int s = scan_launch_dev<int32_t, int32_t>(flag, pos, &cnt[C_V], V0, 0, &cnt[C_EMIT],
+                                                      scan, st);
+            if (s) return s;
+            k_emit<<<gv, 256, 0, st>>>(best, flag, pos, mst, &cnt[C_V], &cnt[C_NMST]);
+            EACB_CHECK_LAUNCH();
+            launches += 3;
+        }
+        k_jump<<<gv, 256, 0, st>>>(color, &cnt[C_V], err);
+        EACB_CHECK_LAUNCH();
+        k_rootflag<<<gv, 256, 0, st>>>(color, flag, &cnt[C_V]);
+        EACB_CHECK_LAUNCH();
+        int s = scan_launch_dev<int32_t, int32_t>(flag, pos, &cnt[C_V], V0, 0, &cnt[C_V_NEXT],
+                                                  scan, st);
+        if (s) return s;
+        k_relabel<<<grid_for(V0, 256), 256, 0, st>>>(label, color, pos, V0);
+        EACB_CHECK_LAUNCH();
+        const int64_t etiles = (Emax + kETile - 1) / kETile;
+        k_round_reset<<<grid_for(V0, 256), 256, 0, st>>>(best, &cnt[C_V_NEXT], scan.status,
+                                                           etiles > 0 ? etiles : 1, scan.counter,
+                                                           &cnt[C_E_NEXT]);
+        EACB_CHECK_LAUNCH();
+        launches += 6;
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        if (timed_filter) {
+            cudaEventCreate(&ev0);
+            cudaEventCreate(&ev1);
+            cudaEventRecord(ev0, st);
+        }
+        SrcEdges se{ea, label, pk, (uint32_t)V0};
+        k_edge_tile<MODE, SrcEdges><<<edge_grid(), kET, 0, st>>>(
+            se, 0, ea, best, scan.status, scan.counter, &cnt[C_E_NEXT], err, &cnt[C_E]);
+        EACB_CHECK_LAUNCH();
+        if (timed_filter) {
+            cudaEventRecord(ev1, st);
+            timed_ev0 = ev0;
+            timed_ev1 = ev1;
+        }
+        k_round_end<<<1, 32, 0, st>>>(cnt, MODE == SEL_MST ? 1 : 0, max_rounds, err, h, use_handle);
+        EACB_CHECK_LAUNCH();
+        launches += 2;
+        if (per_round) *per_round = launches;
+        return EACB_OK;
+    }
+
+    cudaEvent_t timed_ev0 = nullptr, timed_ev1 = nullptr;
+
+    template <int MODE>
+    cudaGraphExec_t round_graph(Pack pk, int *per_round);
+
     // Rounds; edges of round 0 are in `ea` (E0 of them) and `best` holds
-    // their selection.  On return: label = component of every vertex,
-    // *n_comp = number of components, *n_mst = emitted forest edges.
+    // their selection; supervertex ids are [0, V_start) under `label`.  The
+    // rounds run inside one CUDA graph that loops on the device (conditional
+    // WHILE node) until the phase converges; with profiling on (per-launch
+    // CUDA events) or a round limit they are driven from the host instead.
+    // On return: label = component of every vertex, *n_comp = number of
+    // components, *n_mst = forest edges emitted by these rounds.
     template <int MODE>
     int run(Pack pk, int64_t E0, int32_t V_start, cudaStream_t st, int64_t *n_mst_out,
             int64_t *n_comp_out)
     {
-        int32_t V = V_start;
-        int64_t E = E0;
-        int64_t n_mst = 0;
         if (E0 == 0) {                 // nothing to contract: components stay as they are
             *n_mst_out = 0;
             *n_comp_out = V_start;
             return EACB_OK;
         }
-        uint64_t *ein = ea, *eout = ea;          // in-place contraction
-        for (int round = 0; round < max_rounds; ++round) {
-            const unsigned gv = grid_for(V, 256);
-            k_select<MODE><<<gv, 256, 0, st>>>(best, succ, V, label, pk);
-            EACB_CHECK_LAUNCH();
-            k_mirror<<<gv, 256, 0, st>>>(succ, color, MODE == SEL_MST ? flag : nullptr, V);
-            EACB_CHECK_LAUNCH();
-            if (MODE == SEL_MST) {
-                int s = scan_launch<int32_t, int32_t>(flag, pos, V, 0, &cnt[2], scan, st);
+        int64_t before[C_COUNT];
+        EACB_CUDA(cudaMemcpyAsync(before, cnt, sizeof(before), cudaMemcpyDeviceToHost, st));
+        k_round_begin<<<1, 32, 0, st>>>(cnt, V_start, E0);
+        EACB_CHECK_LAUNCH();
+        int per_round = 0;
+        const bool host_driven = prof().enabled != 0 || max_rounds < 96;
+        cudaGraphExec_t exec = host_driven ? nullptr : round_graph<MODE>(pk, &per_round);
+        int64_t after[C_COUNT];
+        int e = 0;
+        if (exec) {
+            EACB_CUDA(cudaGraphLaunch(exec, st));
+            EACB_CUDA(cudaMemcpyAsync(after, cnt, sizeof(after), cudaMemcpyDeviceToHost, st));
+            EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+            EACB_CUDA(cudaStreamSynchronize(st));
+            count_launch((int)(after[C_ROUNDS] * per_round));
+        } else {
+            for (int round = 0; round < max_rounds; ++round) {
+                const bool timed = prof().enabled != 0;
+                int64_t E_in = 0;
+                if (timed)
+                    EACB_CUDA(cudaMemcpyAsync(&E_in, &cnt[C_E], sizeof(int64_t),
+                                              cudaMemcpyDeviceToHost, st));
+                int s = enqueue_round<MODE>(pk, st, 0, 0, timed, &per_round);
                 if (s) return s;
-                k_emit<<<gv, 256, 0, st>>>(best, flag, pos, mst + mst_base + n_mst, V);
-                EACB_CHECK_LAUNCH();
+                EACB_CUDA(cudaMemcpyAsync(after, cnt, sizeof(after), cudaMemcpyDeviceToHost, st));
+                EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+                EACB_CUDA(cudaStreamSynchronize(st));
+                if (timed) {
+                    // algorithmic HBM bytes of one contraction: every edge word
+                    // read once, every surviving edge word written once
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, timed_ev0, timed_ev1);
+                    prof().ms[PROF_EDGE_TILE] += ms;
+                    prof().bytes[PROF_EDGE_TILE] +=
+                        8.0 * (double)E_in + 8.0 * (double)after[C_E_NEXT];
+                    prof().count[PROF_EDGE_TILE] += 1;
+                    cudaEventDestroy(timed_ev0);
+                    cudaEventDestroy(timed_ev1);
+                }
+                if (e || after[C_DONE]) break;
             }
-            k_jump<<<gv, 256, 0, st>>>(color, V, err);
-            EACB_CHECK_LAUNCH();
-            k_rootflag<<<gv, 256, 0, st>>>(color, flag, V);
-            EACB_CHECK_LAUNCH();
-            int s = scan_launch<int32_t, int32_t>(flag, pos, V, 0, &cnt[1], scan, st);
-            if (s) return s;
-            k_relabel<<<grid_for(V0, 256), 256, 0, st>>>(label, color, pos, V0);
-            EACB_CHECK_LAUNCH();
-            EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V, st));
-            SrcEdges se{ein, label, pk, (uint32_t)V0};
-            cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-            const bool timed = prof().enabled != 0;
-            if (timed) {
-                cudaEventCreate(&ev0);
-                cudaEventCreate(&ev1);
-                cudaEventRecord(ev0, st);
-            }
-            s = filter<MODE>(se, E, eout, st);
-            if (s) return s;
-            if (timed) cudaEventRecord(ev1, st);
-            int64_t h[3];
-            s = read_counts(st, h);
-            if (s) return s;
-            if (timed) {
-                // algorithmic HBM bytes of one contraction: every edge word read
-                // once, every surviving edge word written once
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, ev0, ev1);
-                prof().ms[PROF_EDGE_TILE] += ms;
-                prof().bytes[PROF_EDGE_TILE] += 8.0 * (double)E + 8.0 * (double)h[0];
-                prof().count[PROF_EDGE_TILE] += 1;
-                cudaEventDestroy(ev0);
-                cudaEventDestroy(ev1);
-            }
-            if (MODE == SEL_MST) n_mst += h[2];
-            int32_t Vn = (int32_t)h[1];
-            int64_t En = h[0];
-            if (Vn <= 1 || En == 0) {
-                *n_mst_out = n_mst;
-                *n_comp_out = Vn;
-                return EACB_OK;
-            }
-            if (Vn >= V) return EACB_ERR_NOT_CONVERGED;
-            V = Vn;
-            E = En;
         }
-        if (max_rounds < 96) {        // debug trace: stopped on purpose
-            *n_mst_out = n_mst;
-            *n_comp_out = V;
-            return EACB_OK;
+        if (e) return dev_err_to_status(e);
+        const int64_t done = after[C_DONE];
+        if (done == 2) return EACB_ERR_NOT_CONVERGED;                 // no progress
+        if (done == 0 || done == 3) {                                  // round cap
+            if (max_rounds >= 96) return EACB_ERR_NOT_CONVERGED;
         }
-        return EACB_ERR_NOT_CONVERGED;
+        *n_mst_out = after[C_NMST] - before[C_NMST];
+        *n_comp_out = after[C_V];
+        return EACB_OK;
     }
 };
+
+// Cache of instantiated round graphs, keyed by everything the captured
+// kernels see (workspace layout, sizes, mode, key packing, device).
+struct GraphKey {
+    const void *base;
+    int64_t V0, Emax;
+    int mode, vbits, dev, max_rounds;
+    bool operator==(const GraphKey &o) const
+    {
+        return base == o.base && V0 == o.V0 && Emax == o.Emax && mode == o.mode &&
+               vbits == o.vbits && dev == o.dev && max_rounds == o.max_rounds;
+    }
+};
+struct GraphEntry {
+    GraphKey key;
+    cudaGraphExec_t exec;
+    int per_round;
+};
+// One cache per host thread: an entry is only ever launched by the thread
+// that built it, so no other thread can destroy a graph in use.
+struct GraphCache {
+    std::vector<GraphEntry> v;
+    ~GraphCache()
+    {
+        for (auto &g : v) cudaGraphExecDestroy(g.exec);
+    }
+};
+static thread_local GraphCache t_graphs;
+
+// Builds (once per key) the graph: a conditional WHILE node whose body is
+// one round; the body's last kernel clears the condition when the phase has
+// converged.  Returns nullptr if this driver cannot build it (the host then
+// drives the rounds).
+template <int MODE>
+cudaGraphExec_t Engine::round_graph(Pack pk, int *per_round)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    GraphKey key{(const void *)err, V0, Emax, MODE, pk.vbits, dev, max_rounds};
+    for (auto &g : t_graphs.v)
+        if (g.key == key) {
+            *per_round = g.per_round;
+            return g.exec;
+        }
+    cudaStream_t cs = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int pr = 0;
+    bool ok = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaGraphCreate(&graph, 0) == cudaSuccess;
+    cudaGraphConditionalHandle h = 0;
+    if (ok) ok = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) ==
+                 cudaSuccess;
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t node = nullptr;
+    if (ok) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        ok = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
+    }
+    if (ok) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        ok = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            const int s = enqueue_round<MODE>(pk, cs, 1, h, false, &pr);
+            count_launch(-pr);                // capturing launches nothing
+            cudaGraph_t out = nullptr;
+            ok = cudaStreamEndCapture(cs, &out) == cudaSuccess && s == EACB_OK;
+        }
+    }
+    if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (cs) cudaStreamDestroy(cs);
+    cudaGetLastError();                       // a failed build leaves no sticky error
+    if (!ok) {
+        if (exec) cudaGraphExecDestroy(exec);
+        return nullptr;
+    }
+    if (t_graphs.v.size() >= 16) {
+        cudaGraphExecDestroy(t_graphs.v.front().exec);
+        t_graphs.v.erase(t_graphs.v.begin());
+    }
+    t_graphs.v.push_back(GraphEntry{key, exec, pr});
+    *per_round = pr;
+    return exec;
+}
 
 static int g_debug_rounds = 0;   // 0 = off; else rounds to run (round-trace test entry)
 
@@ -880,7 +1112,7 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
             if (E == 0) return EACB_OK;
             k_phase_csr<WT><<<gr, 256, 0, st>>>(first, deg, dest, weight, V, E, wbits, lo, hi,
                                                 g.label, pk, g.ea,
-                                                (unsigned long long *)&g.cnt[3], g.best, g.err);
+                                                (unsigned long long *)&g.cnt[C_CURSOR], g.best, g.err);
             EACB_CHECK_LAUNCH();
             return EACB_OK;
         };
@@ -1149,7 +1381,7 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
         if (nnz == 0) return EACB_OK;
         k_phase_upper<<<grid_for((int64_t)n * 32, 256), 256, 0, st>>>(
             indptr, indices, diassoc, n, nnz, lo, hi, g.label, pk, g.ea,
-            (unsigned long long *)&g.cnt[3], g.best, g.err);
+            (unsigned long long *)&g.cnt[C_CURSOR], g.best, g.err);
         EACB_CHECK_LAUNCH();
         return EACB_OK;
     };

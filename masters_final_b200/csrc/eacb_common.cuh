@@ -230,7 +230,8 @@ struct Prof {
     int64_t count[PROF_NTAGS];
 };
 Prof &prof();
-inline void count_launch(int n) { prof().launches += n; }
+// the launch counter is shared by every host thread that calls the library
+inline void count_launch(int n) { __atomic_fetch_add(&prof().launches, (int64_t)n, __ATOMIC_RELAXED); }
 
 // Times one launch when profiling is on: construct before the launch,
 // call done(bytes) after it.  Synchronizes on the end event.

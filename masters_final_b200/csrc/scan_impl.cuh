@@ -37,13 +37,21 @@ __device__ __forceinline__ int32_t narrow<int32_t>(int64_t v) { return (int32_t)
 template <typename TIn, typename TOut, bool VEC>
 __global__ void __launch_bounds__(kScanThreads)
 k_scan(const TIn *__restrict__ in, TOut *__restrict__ out, int64_t n, int64_t init,
-       uint64_t *status, int *counter, int64_t *total, int *err)
+       uint64_t *status, int *counter, int64_t *total, int *err, const int64_t *d_n = nullptr)
 {
     __shared__ int s_tile;
     __shared__ int64_t s_prefix;
+    // with d_n the length is read on the device and the grid is sized for
+    // the largest length: surplus blocks take tile ids past the end and leave
+    if (d_n) n = *d_n;
     if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
     __syncthreads();
     const int64_t tile = s_tile;
+    if (tile * kScanTile >= n && !(n == 0 && tile == 0)) return;
+    if (n == 0) {
+        if (threadIdx.x == 0 && total) *total = init;
+        return;
+    }
     const int64_t base = tile * kScanTile + (int64_t)threadIdx.x * kScanItems;
     TIn v[kScanItems];
     const bool full = base + kScanItems <= n;
@@ -95,6 +103,29 @@ k_scan(const TIn *__restrict__ in, TOut *__restrict__ out, int64_t n, int64_t in
 }
 
 __global__ void k_set_i64(int64_t *p, int64_t v);
+
+// Clears look-back state with a kernel (usable where memset nodes are not).
+__global__ void k_clear_status(uint64_t *status, int64_t n, int *counter);
+
+// Scan whose length is read on the device (*d_n <= max_n); no memset calls,
+// so it can be captured into a conditional graph body.
+template <typename TIn, typename TOut>
+inline int scan_launch_dev(const TIn *in, TOut *out, const int64_t *d_n, int64_t max_n,
+                           int64_t init, int64_t *d_total, const ScanScratch &s, cudaStream_t st)
+{
+    const int64_t ntiles = (max_n + kScanTile - 1) / kScanTile;
+    const int64_t grid = ntiles > 0 ? ntiles : 1;
+    k_clear_status<<<grid_for(grid, 256, 148 * 4), 256, 0, st>>>(s.status, grid, s.counter);
+    EACB_CHECK_LAUNCH();
+    if (((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0))
+        k_scan<TIn, TOut, true><<<(unsigned)grid, kScanThreads, 0, st>>>(
+            in, out, max_n, init, s.status, s.counter, d_total, s.err, d_n);
+    else
+        k_scan<TIn, TOut, false><<<(unsigned)grid, kScanThreads, 0, st>>>(
+            in, out, max_n, init, s.status, s.counter, d_total, s.err, d_n);
+    EACB_CHECK_LAUNCH();
+    return EACB_OK;
+}
 
 template <typename TIn, typename TOut>
 inline int scan_launch(const TIn *in, TOut *out, int64_t n, int64_t init, int64_t *d_total,

@@ -67,3 +67,13 @@ extern "C" void eacb_profile_read(int64_t *launches, double *ms, double *bytes, 
         if (count) count[i] = eacb::prof().count[i];
     }
 }
+
+namespace eacb {
+__global__ void k_clear_status(uint64_t *status, int64_t n, int *counter)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        status[i] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *counter = 0;
+}
+}  // namespace eacb

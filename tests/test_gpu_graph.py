@@ -110,6 +110,30 @@ def test_boruvka_knn_1m_properties(T):
     _check_mst(indptr, dest, w, mst, n)
 
 
+def test_rounds_graph_vs_host_driven(T):
+    """The rounds run as one device-looping CUDA graph by default and from
+    the host with profiling on; both give the same forest and components,
+    and repeated calls reuse the cached graph."""
+    from masters_final_b200 import _lib, workloads as W
+    from masters_final_b200.graph.mst import boruvka_minho_gpu
+    from masters_final_b200.graph.connected_components import connected_comps_gpu
+    indptr, dest, w = W.knn_graph(200_000, k=8, seed=11)
+    first, deg = indptr[:-1].astype(np.int32), np.diff(indptr).astype(np.int32)
+    runs = []
+    for prof in (False, True, False):
+        _lib.profile_enable(prof)
+        try:
+            mst, n = boruvka_minho_gpu(dest, w, first, deg)
+            cc = connected_comps_gpu(dest, w, first, deg)
+        finally:
+            _lib.profile_enable(False)
+        runs.append((np.sort(mst[:n]), cc))
+    for mst, cc in runs[1:]:
+        assert np.array_equal(mst, runs[0][0])
+        assert np.array_equal(cc, runs[0][1])
+    _check_mst(indptr, dest, w, runs[0][0], runs[0][0].size)
+
+
 @pytest.mark.parametrize("dt", [np.uint16, np.int32, np.float32])
 def test_boruvka_weight_types(T, dt):
     from masters_final_b200 import workloads as W
