@@ -119,85 +119,25 @@ __device__ __forceinline__ int64_t block_sum(int64_t v)
 
 // Stream the tails of all partitions into [j0, jl): calls op(j) per element.
 // Cursor ts[p] advances past consumed elements.
-// Stream the tails of all partitions into [j0, jl): calls op(j) per element
-// and advances the cursors ts[p].  Called by the whole block.  The elements
-// below jl of all P tails are laid out as one flat range (a binary search per
-// tail finds its part, a scan gives the offsets) and the block walks it in
-// warp-contiguous 32-element pieces, several pieces per warp in flight, so
-// the member-list reads are coalesced and the work is balanced however
-// uneven the tails are.
 template <typename Op>
 __device__ __forceinline__ void stream_chunk(const int32_t *members, int64_t *ts, const int64_t *te,
-                                             int32_t P, int32_t jl, int32_t *s_len,
-                                             int32_t *s_off, Op op)
+                                             int32_t P, int32_t jl, Op op)
 {
-    for (int p = threadIdx.x; p < P; p += blockDim.x) {
-        int64_t lo = ts[p], hi = te[p];
-        while (lo < hi) {
-            const int64_t mid = (lo + hi) >> 1;
-            if (members[mid] < jl) lo = mid + 1; else hi = mid;
-        }
-        s_len[p] = (int32_t)(lo - ts[p]);
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        int v[8];
-        int sum = 0;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int p = lane * 8 + q;
-            v[q] = p < P ? s_len[p] : 0;
-            sum += v[q];
-        }
-        int incl = sum;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int o = __shfl_up_sync(0xffffffffu, incl, d);
-            if (lane >= d) incl += o;
-        }
-        int run = incl - sum;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int p = lane * 8 + q;
-            if (p < P) s_off[p] = run;
-            run += v[q];
-        }
-        if (lane == 31) s_off[P] = incl;
-    }
-    __syncthreads();
-    const int32_t T = s_off[P];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    constexpr int U = 4;
-    for (int32_t c0 = warp * 32 * U; c0 < T; c0 += nw * 32 * U) {
-        int32_t jv[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int32_t piece = c0 + u * 32;
-            jv[u] = -1;
-            if (piece < T) {
-                // partition of the piece's first element: largest p with
-                // s_off[p] <= piece (skips empty tails), then each lane walks on
-                int lo = 0, hi = P;
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (s_off[mid] <= piece) lo = mid; else hi = mid;
-                }
-                const int32_t f = piece + lane;
-                if (f < T) {
-                    int p = lo;
-                    while (s_off[p + 1] <= f) ++p;
-                    jv[u] = members[ts[p] + (f - s_off[p])];
-                }
-            }
+    for (int p = warp; p < P; p += nw) {
+        int64_t cur = ts[p];
+        const int64_t end = te[p];
+        while (cur < end) {
+            const int64_t idx = cur + lane;
+            const int32_t j = idx < end ? members[idx] : 0x7fffffff;
+            const bool ok = j < jl;
+            const unsigned bal = __ballot_sync(0xffffffffu, ok);
+            if (ok) op(j);
+            cur += __popc(bal);
+            if (bal != 0xffffffffu) break;
         }
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-            if (jv[u] >= 0) op(jv[u]);
+        if (lane == 0) ts[p] = cur;
     }
-    __syncthreads();
-    for (int p = threadIdx.x; p < P; p += blockDim.x) ts[p] += s_len[p];
-    __syncthreads();
 }
 
 // ---------------------------------------------------------------- pass 1 --
@@ -207,7 +147,6 @@ k_rows_count(TailCtx tc, const int32_t *order, const int64_t *cap_indptr, int32_
 {
     extern __shared__ uint32_t bm[];
     __shared__ int64_t ts[kMaxP], te[kMaxP];
-    __shared__ int32_t s_len[kMaxP], s_off[kMaxP + 1];
     __shared__ int s_row;
     const int32_t n = tc.n, P = tc.P;
     constexpr int32_t kCols = kBitmapBytes * 8;
@@ -230,7 +169,7 @@ k_rows_count(TailCtx tc, const int32_t *order, const int64_t *cap_indptr, int32_
             for (int w = threadIdx.x; w < nwords; w += blockDim.x) bm[w] = 0;
             __syncthreads();
             const int32_t jb = (int32_t)j0;
-            stream_chunk(tc.members, ts, te, P, jl, s_len, s_off, [&](int32_t j) {
+            stream_chunk(tc.members, ts, te, P, jl, [&](int32_t j) {
                 const int32_t o = j - jb;
                 atomicOr(&bm[o >> 5], 1u << (o & 31));
             });
@@ -299,7 +238,6 @@ k_rows_fill(TailCtx tc, const int32_t *rowflag, const int64_t *indptr, int32_t *
 {
     extern __shared__ uint32_t ctr32[];
     __shared__ int64_t ts[kMaxP], te[kMaxP];
-    __shared__ int32_t s_len[kMaxP], s_off[kMaxP + 1];
     __shared__ int s_row;
     const int32_t n = tc.n, P = tc.P;
     constexpr int32_t kCols = kCountBytes;
@@ -323,7 +261,7 @@ k_rows_fill(TailCtx tc, const int32_t *rowflag, const int64_t *indptr, int32_t *
             for (int w = threadIdx.x; w < nwords; w += blockDim.x) ctr32[w] = 0;
             __syncthreads();
             const int32_t jb = (int32_t)j0;
-            stream_chunk(tc.members, ts, te, P, jl, s_len, s_off, [&](int32_t j) {
+            stream_chunk(tc.members, ts, te, P, jl, [&](int32_t j) {
                 const int32_t o = j - jb;
                 atomicAdd(&ctr32[o >> 2], 1u << (8 * (o & 3)));
             });
