@@ -27,9 +27,10 @@
 //  3. pass 2, same streaming into shared-memory byte counters (one byte per
 //     column, four packed per word), then a block-wide compaction of the
 //     non-zero counters writes the row in column order straight into the
-//     final CSR.  Rows whose distinct count exceeds their capacity (rare)
-//     are redone by a rank-aware kernel that streams partitions in
-//     processing order and applies the keep rule.
+//     final CSR.  Rows whose distinct count exceeds their capacity are
+//     redone by a rank-aware kernel: a column's rank (first partition in
+//     processing order that associates it) is an atomicMin per visit, and
+//     the keep rule is applied from the rank histogram.
 #include "eacb_common.cuh"
 #include "scan_impl.cuh"
 #include "members.cuh"
@@ -40,7 +41,8 @@ constexpr int kMaxK = 8192;            // largest cluster id + 1 supported
 constexpr int kRowThreads = 512;
 constexpr int kBitmapBytes = 96 * 1024;        // pass 1: 786,432 columns per chunk
 constexpr int kCountBytes = 96 * 1024;         // pass 2: 98,304 columns per chunk
-constexpr int kCapBytes = 48 * 1024;           // capped rows: counts + ranks
+constexpr int kCapCols = 16 * 1024;            // capped rows: columns per chunk
+constexpr int kCapSmem = kCapCols * 5;         // byte counters + 32-bit ranks
 constexpr int kMaxP = 255;
 
 struct CoWS {
@@ -117,8 +119,13 @@ __device__ __forceinline__ int64_t block_sum(int64_t v)
     return tot;
 }
 
-// Stream the tails of all partitions into [j0, jl): calls op(j) per element.
-// Cursor ts[p] advances past consumed elements.
+// Stream the tails of all partitions into [j0, jl): calls op(j, p) per
+// element j of tail p, and advances the cursors ts[p] past what it consumed.
+// A warp walks one tail at a time, kStreamU x 32 members per step with all
+// loads issued before any is used (the walk is latency-bound: a tail
+// averages a few hundred members); a tail is sorted, so the members below jl
+// are a prefix of the step.
+constexpr int kStreamU = 8;
 template <typename Op>
 __device__ __forceinline__ void stream_chunk(const int32_t *members, int64_t *ts, const int64_t *te,
                                              int32_t P, int32_t jl, Op op)
@@ -128,13 +135,21 @@ __device__ __forceinline__ void stream_chunk(const int32_t *members, int64_t *ts
         int64_t cur = ts[p];
         const int64_t end = te[p];
         while (cur < end) {
-            const int64_t idx = cur + lane;
-            const int32_t j = idx < end ? members[idx] : 0x7fffffff;
-            const bool ok = j < jl;
-            const unsigned bal = __ballot_sync(0xffffffffu, ok);
-            if (ok) op(j);
-            cur += __popc(bal);
-            if (bal != 0xffffffffu) break;
+            int32_t j[kStreamU];
+#pragma unroll
+            for (int u = 0; u < kStreamU; ++u) {
+                const int64_t idx = cur + u * 32 + lane;
+                j[u] = idx < end ? __ldg(members + idx) : 0x7fffffff;
+            }
+            int taken = 0;
+#pragma unroll
+            for (int u = 0; u < kStreamU; ++u) {
+                const bool ok = j[u] < jl;
+                if (ok) op(j[u], p);
+                taken += __popc(__ballot_sync(0xffffffffu, ok));
+            }
+            cur += taken;
+            if (taken != kStreamU * 32) break;
         }
         if (lane == 0) ts[p] = cur;
     }
@@ -169,7 +184,7 @@ k_rows_count(TailCtx tc, const int32_t *order, const int64_t *cap_indptr, int32_
             for (int w = threadIdx.x; w < nwords; w += blockDim.x) bm[w] = 0;
             __syncthreads();
             const int32_t jb = (int32_t)j0;
-            stream_chunk(tc.members, ts, te, P, jl, [&](int32_t j) {
+            stream_chunk(tc.members, ts, te, P, jl, [&](int32_t j, int) {
                 const int32_t o = j - jb;
                 atomicOr(&bm[o >> 5], 1u << (o & 31));
             });
@@ -261,7 +276,7 @@ k_rows_fill(TailCtx tc, const int32_t *rowflag, const int64_t *indptr, int32_t *
             for (int w = threadIdx.x; w < nwords; w += blockDim.x) ctr32[w] = 0;
             __syncthreads();
             const int32_t jb = (int32_t)j0;
-            stream_chunk(tc.members, ts, te, P, jl, [&](int32_t j) {
+            stream_chunk(tc.members, ts, te, P, jl, [&](int32_t j, int) {
                 const int32_t o = j - jb;
                 atomicAdd(&ctr32[o >> 2], 1u << (8 * (o & 3)));
             });
@@ -278,130 +293,124 @@ k_rows_fill(TailCtx tc, const int32_t *rowflag, const int64_t *indptr, int32_t *
 }
 
 // ------------------------------------------------------ rows over capacity --
-// One CTA per flagged row.  Partitions are streamed in processing order with
-// a barrier between partitions, so the first partition that touches a
-// column is its rank.
+// One CTA per flagged row.  The tails are indexed by processing position q
+// (tail q is partition order[q]); a column's rank is the smallest q whose
+// tail holds it, i.e. the first partition in processing order that
+// associates it with the row -- an atomicMin per visit, so all tails stream
+// at once as in the other passes.  Pass 0 histograms the ranks; the keep rule
+// then needs r* (the rank at which the running distinct count reaches the
+// capacity) and the quota of rank-r* columns that still fit; pass 1 keeps
+// rank < r* and the first `quota` rank-r* columns in column order.  A row
+// whose tail span fits one chunk keeps its pass-0 chunk for pass 1.
 __global__ void __launch_bounds__(kRowThreads)
 k_rows_capped(TailCtx tc, const int32_t *order, const int32_t *rowflag, const int64_t *cap_indptr,
               const int64_t *indptr, int32_t *indices, uint8_t *data, int *queue, int *gmax,
               unsigned long long *disc, int *err)
 {
     extern __shared__ uint32_t sm[];
-    uint32_t *ctr32 = sm;                                  // kCapBytes counters
-    uint8_t *rank = (uint8_t *)(sm + kCapBytes / 4);       // kCapBytes ranks
+    uint32_t *ctr32 = sm;                      // kCapCols byte counters
+    uint32_t *rank = sm + kCapCols / 4;        // kCapCols ranks (kNoRank: column untouched)
+    constexpr uint32_t kNoRank = 0xffffffffu;
     __shared__ int64_t ts[kMaxP], te[kMaxP];
     __shared__ int hist[kMaxP + 1];
     __shared__ int s_row, s_rstar, s_quota, s_seen;
-    __shared__ int64_t s_end;
     const int32_t n = tc.n, P = tc.P;
-    constexpr int32_t kCols = kCapBytes;
     int maxc = 0;
     while (true) {
         const int i = next_row(queue, &s_row);
         if (i >= n) break;
         if (!rowflag[i]) continue;
         const int64_t cap = cap_indptr[i + 1] - cap_indptr[i];
+        const bool one_chunk = (int64_t)n - ((int64_t)i + 1) <= kCapCols;
         for (int q = threadIdx.x; q <= P; q += blockDim.x) hist[q] = 0;
-        int s_rs = 0, s_qt = 0;
+        int rs = 0, qt = 0;
         int64_t out = indptr[i];
         unsigned long long dsum = 0;
         for (int pass = 0; pass < 2; ++pass) {
-            for (int q = threadIdx.x; q < P; q += blockDim.x) {
-                int64_t s, e;
-                tc.tail(i, order[q], s, e);
-                ts[q] = s;
-                te[q] = e;
-            }
+            const bool stream = pass == 0 || !one_chunk;
+            if (stream)
+                for (int q = threadIdx.x; q < P; q += blockDim.x) {
+                    int64_t s, e;
+                    tc.tail(i, order[q], s, e);
+                    ts[q] = s;
+                    te[q] = e;
+                }
             if (threadIdx.x == 0) s_seen = 0;
             __syncthreads();
-            for (int64_t j0 = (int64_t)i + 1; j0 < n; j0 += kCols) {
-                const int32_t jl = (int32_t)((j0 + kCols < n) ? j0 + kCols : n);
+            for (int64_t j0 = (int64_t)i + 1; j0 < n; j0 += kCapCols) {
+                const int32_t jl = (int32_t)((j0 + kCapCols < n) ? j0 + kCapCols : n);
                 const int width = (int)(jl - j0);
-                const int nw = (width + 15) >> 4 << 2;
-                for (int w = threadIdx.x; w < nw; w += blockDim.x) {
-                    ctr32[w] = 0;
-                    reinterpret_cast<uint32_t *>(rank)[w] = 0xffffffffu;
-                }
-                __syncthreads();
-                for (int q = 0; q < P; ++q) {
-                    // end of this partition's run inside the chunk
-                    if (threadIdx.x == 0) {
-                        int64_t lo = ts[q], hi = te[q];
-                        while (lo < hi) {
-                            int64_t mid = (lo + hi) >> 1;
-                            if (tc.members[mid] < jl) lo = mid + 1; else hi = mid;
-                        }
-                        s_end = lo;
-                    }
+                if (stream) {
+                    const int nw = (width + 15) >> 4 << 2;
+                    for (int w = threadIdx.x; w < nw; w += blockDim.x) ctr32[w] = 0;
+                    for (int o = threadIdx.x; o < width; o += blockDim.x) rank[o] = kNoRank;
                     __syncthreads();
-                    for (int64_t idx = ts[q] + threadIdx.x; idx < s_end; idx += blockDim.x) {
-                        const int32_t o = tc.members[idx] - (int32_t)j0;
-                        const uint32_t old = atomicAdd(&ctr32[o >> 2], 1u << (8 * (o & 3)));
-                        if (((old >> (8 * (o & 3))) & 255u) == 0) rank[o] = (uint8_t)q;
-                    }
-                    __syncthreads();
-                    if (threadIdx.x == 0) ts[q] = s_end;
+                    const int32_t jb = (int32_t)j0;
+                    stream_chunk(tc.members, ts, te, P, jl, [&](int32_t j, int q) {
+                        const int32_t o = j - jb;
+                        atomicAdd(&ctr32[o >> 2], 1u << (8 * (o & 3)));
+                        atomicMin(&rank[o], (uint32_t)q);
+                    });
                     __syncthreads();
                 }
                 if (pass == 0) {
                     for (int o = threadIdx.x; o < width; o += blockDim.x)
-                        if (rank[o] != 0xff) atomicAdd(&hist[rank[o]], 1);
+                        if (rank[o] != kNoRank) atomicAdd(&hist[rank[o]], 1);
                     __syncthreads();
-                } else {
-                    // kept: rank < r*, or rank == r* among the first `quota`
-                    // such columns in column order
-                    const int nvec = (width + 15) >> 4;
-                    const int per = (nvec + blockDim.x - 1) / blockDim.x;
-                    const int o0 = threadIdx.x * per * 16, o1 = min(width, o0 + per * 16);
-                    int mystar = 0;
-                    for (int o = o0; o < o1; ++o) mystar += (rank[o] == s_rs);
-                    int64_t tstar;
-                    int64_t before = s_seen + block_excl_sum<kRowThreads>(mystar, tstar);
-                    int64_t seen = before;
-                    const uint8_t *c8 = (const uint8_t *)ctr32;
-                    int kept = 0;
-                    for (int o = o0; o < o1; ++o) {
-                        const int r = rank[o];
-                        if (r == 0xff) continue;
-                        bool k = r < s_rs || (r == s_rs && seen < s_qt);
-                        if (r == s_rs) seen++;
-                        if (k) kept++; else dsum += c8[o];
-                    }
-                    int64_t tk;
-                    int64_t at = out + block_excl_sum<kRowThreads>(kept, tk);
-                    seen = before;
-                    for (int o = o0; o < o1; ++o) {
-                        const int r = rank[o];
-                        if (r == 0xff) continue;
-                        bool k = r < s_rs || (r == s_rs && seen < s_qt);
-                        if (r == s_rs) seen++;
-                        if (k) {
-                            indices[at] = (int32_t)j0 + o;
-                            data[at] = c8[o];
-                            maxc = max(maxc, (int)c8[o]);
-                            at++;
-                        }
-                    }
-                    out += tk;
-                    __syncthreads();
-                    if (threadIdx.x == 0) s_seen += (int)tstar;
-                    __syncthreads();
+                    continue;
                 }
+                // kept: rank < r*, or rank == r* among the first `quota` such
+                // columns in column order; each thread owns a contiguous run
+                const int per = (width + blockDim.x - 1) / blockDim.x;
+                const int o0 = min(width, (int)threadIdx.x * per), o1 = min(width, o0 + per);
+                int mystar = 0;
+                for (int o = o0; o < o1; ++o) mystar += (rank[o] == (uint32_t)rs);
+                int64_t tstar;
+                const int64_t before = s_seen + block_excl_sum<kRowThreads>(mystar, tstar);
+                int64_t seen = before;
+                const uint8_t *c8 = (const uint8_t *)ctr32;
+                int kept = 0;
+                for (int o = o0; o < o1; ++o) {
+                    const uint32_t r = rank[o];
+                    if (r == kNoRank) continue;
+                    const bool k = r < (uint32_t)rs || (r == (uint32_t)rs && seen < qt);
+                    if (r == (uint32_t)rs) seen++;
+                    if (k) kept++; else dsum += c8[o];
+                }
+                int64_t tk;
+                int64_t at = out + block_excl_sum<kRowThreads>(kept, tk);
+                seen = before;
+                for (int o = o0; o < o1; ++o) {
+                    const uint32_t r = rank[o];
+                    if (r == kNoRank) continue;
+                    const bool k = r < (uint32_t)rs || (r == (uint32_t)rs && seen < qt);
+                    if (r == (uint32_t)rs) seen++;
+                    if (k) {
+                        indices[at] = (int32_t)j0 + o;
+                        data[at] = c8[o];
+                        maxc = max(maxc, (int)c8[o]);
+                        at++;
+                    }
+                }
+                out += tk;
+                __syncthreads();
+                if (threadIdx.x == 0) s_seen += (int)tstar;
+                __syncthreads();
             }
             if (pass == 0) {
                 if (threadIdx.x == 0) {
                     int64_t cum = 0;
-                    int rs = P, qt = 0;
+                    int r = P, quota = 0;
                     for (int q = 0; q < P; ++q) {
-                        if (cum + hist[q] >= cap) { rs = q; qt = (int)(cap - cum); break; }
+                        if (cum + hist[q] >= cap) { r = q; quota = (int)(cap - cum); break; }
                         cum += hist[q];
                     }
-                    s_rstar = rs;
-                    s_quota = qt;
+                    s_rstar = r;
+                    s_quota = quota;
                 }
                 __syncthreads();
-                s_rs = s_rstar;
-                s_qt = s_quota;
+                rs = s_rstar;
+                qt = s_quota;
             }
         }
         if (threadIdx.x == 0 && out != indptr[i + 1]) set_err(err, DEV_CAPACITY);
@@ -483,8 +492,7 @@ extern "C" int eacb_coassoc_prepare(const int32_t *labels, int32_t n, int32_t P,
     if ((s = scan_launch<int32_t, int64_t>(w.cnt, w.S, m, 0, &w.S[m], w.scan, st))) return s;
     const size_t place_smem = (size_t)K * (sizeof(int64_t) + sizeof(int32_t));
     if (place_smem > 48 * 1024)
-        EACB_CUDA(cudaFuncSetAttribute(k_ml_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)place_smem));
+        EACB_CUDA(allow_max_dyn_smem(k_ml_place));
     k_ml_place<<<(unsigned)(P * nt), 32, place_smem, st>>>(labels, n, K, nt, w.S, w.members,
                                                            w.mypos);
     EACB_CHECK_LAUNCH();
@@ -513,8 +521,7 @@ extern "C" int eacb_coassoc_count(const int32_t *labels, int32_t n, int32_t P, i
     if (c.overflow) return EACB_ERR_WORKSPACE;
     EACB_CUDA(cudaMemsetAsync(w.queue, 0, 4 * sizeof(int), st));
     TailCtx tc{labels, w.members, w.mypos, w.S, n, P, K, w.ntiles};
-    EACB_CUDA(cudaFuncSetAttribute(k_rows_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   kBitmapBytes));
+    EACB_CUDA(allow_max_dyn_smem(k_rows_count));
     ProfScope ps(PROF_COASSOC, st);
     k_rows_count<<<row_grid(), kRowThreads, kBitmapBytes, st>>>(tc, w.order, cap_indptr, w.rowcnt,
                                                                  w.rowflag, &w.queue[0], w.err);
@@ -612,16 +619,14 @@ extern "C" int eacb_coassoc_fill(const int32_t *labels, int32_t n, int32_t P, in
     EACB_CUDA(cudaMemsetAsync(w.disc, 0, sizeof(unsigned long long), st));
     EACB_CUDA(cudaMemsetAsync(w.maxcnt, 0, sizeof(int), st));
     TailCtx tc{labels, w.members, w.mypos, w.S, n, P, K, w.ntiles};
-    EACB_CUDA(cudaFuncSetAttribute(k_rows_fill, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   kCountBytes));
-    EACB_CUDA(cudaFuncSetAttribute(k_rows_capped, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   2 * kCapBytes));
+    EACB_CUDA(allow_max_dyn_smem(k_rows_fill));
+    EACB_CUDA(allow_max_dyn_smem(k_rows_capped));
     ProfScope ps(PROF_COASSOC, st);
     k_rows_fill<<<row_grid(), kRowThreads, kCountBytes, st>>>(tc, w.rowflag, indptr, indices, data,
                                                                &w.queue[1], w.maxcnt, w.err);
     EACB_CHECK_LAUNCH();
     ps.done(0.0);
-    k_rows_capped<<<row_grid(), kRowThreads, 2 * kCapBytes, st>>>(
+    k_rows_capped<<<row_grid(), kRowThreads, kCapSmem, st>>>(
         tc, w.order, w.rowflag, cap_indptr, indptr, indices, data, &w.queue[2], w.maxcnt, w.disc,
         w.err);
     EACB_CHECK_LAUNCH();

@@ -67,6 +67,7 @@ def _random_labels(rng, P, n, kmin, kmax, holes=0.0):
     (3, 4000, 12, 30, 300, 2, "constant", 0.05),    # -1 labels, constant caps
     (4, 200_000, 6, 3000, 4000, 3, "linear", 0.0),  # several column chunks per row
     (5, 2500, 255, 10, 20, 3, "linear", 0.0),       # maximum ensemble size
+    (6, 36_000, 5, 30, 50, 1, "linear", 0.0),       # capped rows over several chunks
 ])
 def test_coassoc_vs_oracle(T, seed, n, P, kmin, kmax, factor, kind, holes):
     rng = np.random.default_rng(seed)
