@@ -14,9 +14,13 @@
  *     256-byte aligned; the library never allocates device memory;
  *   - functions return an eacb_status (0 = success, negative = error) and
  *     never throw; outputs are undefined after an error;
- *   - functions whose work has data-dependent rounds (Boruvka, connected
- *     components, final clustering) synchronize `stream` once per round to
- *     read a few counters; all others are asynchronous on `stream`.
+ *   - functions whose work has data-dependent sizes (Boruvka, connected
+ *     components, co-association, k-means, final clustering) synchronize
+ *     `stream` a few times per call to read counters (Boruvka rounds loop on
+ *     the device inside one CUDA graph per weight phase); the scans are
+ *     asynchronous on `stream`;
+ *   - entry points may be called from several host threads at once on
+ *     different streams and workspaces (eacb_scan_excl_i32_noalloc excepted).
  */
 #ifndef EACB200_H
 #define EACB200_H
@@ -53,6 +57,10 @@ typedef enum {
 
 int eacb_version(void);
 const char *eacb_status_string(int status);
+
+/* After EACB_ERR_CUDA: the cudaError_t of the failed runtime call, on the
+ * calling thread, and the library source file and line that made it. */
+int eacb_last_cuda_error(const char **file, int *line);
 
 /* Every workspace starts with a device error word that asynchronous entry
  * points set on a device-side failure.  Synchronizes `stream`, returns the
@@ -246,6 +254,63 @@ int eacb_final_clustering(const int64_t *indptr, const int32_t *indices,
                           int32_t *labels, int64_t *host_n_fclusts,
                           int32_t *host_labels_valid,
                           void *ws, size_t ws_bytes, uintptr_t stream);
+
+/* ------------------------------------------------------------------------
+ * Batched EAC: many independent instances, each the whole path above
+ * (eacb_kmeans_ensemble -> eacb_coassoc_prepare/count/fill with the
+ * dissimilarity transform -> eacb_final_clustering), in one call.
+ * Replaces the reference's per-dataset loop over generateEnsemble
+ * (MyML/MyML/utils/partition.py:88-124), EAC.buildMatrix
+ * (MyML/MyML/EAC/eac.py:115-140) and EAC.finalClustering (:142-179), as its
+ * experiment drivers run it (experiments/study_kmin.py:398-587).
+ * Per instance the caller gives device X (n x d float32), k (P int32) and
+ * init (P*kmax int32) drawn like the reference, and a device labels array
+ * (n int32).  Results per instance: labels (numbered by smallest member;
+ * all 0 when the lifetime rule yields one cluster, where the reference
+ * returns an empty array), n_fclusts, labels_valid, nnz, nnz_discarded and
+ * status.  The workspace holds n_workers fixed slices
+ * (eacb_batched_workspace_size) and, after them, an arena for the
+ * count-dependent arrays of the instances in flight (at least the largest
+ * instance's co-association CSR plus its final-clustering workspace; more
+ * lets more instances run at once).  ws must be 256-byte aligned.
+ * n_workers host threads, each with its own stream, take the instances
+ * largest first.  The call returns when every instance is done: EACB_OK, or
+ * the status of the first failed instance in input order.
+ * ------------------------------------------------------------------------ */
+typedef struct eacb_instance {
+    const float *X;           /* in: device, n x d row-major */
+    const int32_t *k;         /* in: device, clusters per partition (P) */
+    const int32_t *init;      /* in: device, initial sample indices (P x kmax) */
+    int32_t *labels;          /* out: device, final labels (n) */
+    int32_t n, d, P, kmax;    /* in: d <= 32, P <= 255, kmax <= 8192 */
+    int64_t n_fclusts;        /* out */
+    int64_t nnz;              /* out: co-association entries kept */
+    int64_t nnz_discarded;    /* out */
+    int32_t labels_valid;     /* out */
+    int32_t status;           /* out: eacb status of this instance */
+    float ms_ensemble;        /* out: host wall-clock ms of each stage on its worker */
+    float ms_coassoc;
+    float ms_final;
+    int32_t worker;           /* out: the worker that ran the instance */
+    int32_t cuda_error;       /* out: after EACB_ERR_CUDA, the cudaError_t ... */
+    int32_t cuda_line;        /* ... and the source line of the failed call */
+} eacb_instance;
+
+typedef struct eacb_batch_options {
+    int32_t max_iter;          /* Lloyd label passes (the reference's iters, 3) */
+    float tol;                 /* inertia tolerance (1e-4) */
+    int32_t label_mode;        /* 0 float32 cores, 1 tcgen05 (both exact) */
+    int32_t centroid_mode;     /* 0 float32 point-order sums, 1 float64 */
+    int32_t cap_mode;          /* 0 indptr_linear, 1 indptr_constant */
+    int32_t max_assocs_factor; /* max_assocs = factor * largest cluster (3) */
+    double n_s, n_e, val_s, val_e;  /* indptr_linear parameters (0.05, 1, 1, 0.05) */
+    int32_t n_clusters;        /* 0 = lifetime rule */
+    int32_t reserved;
+} eacb_batch_options;
+
+size_t eacb_batched_workspace_size(const eacb_instance *inst, int32_t n_inst, int32_t n_workers);
+int eacb_batched_eac(eacb_instance *inst, int32_t n_inst, const eacb_batch_options *opt,
+                     int32_t n_workers, void *ws, size_t ws_bytes, uintptr_t stream);
 
 #ifdef __cplusplus
 }

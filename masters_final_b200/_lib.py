@@ -21,9 +21,17 @@ ERR_FIRST_OVERFLOW = -7
 _lib = None
 
 class EACBError(RuntimeError):
-    def __init__(self, status, where):
+    def __init__(self, status, where, cuda=None):
         self.status = status
-        super().__init__("%s failed: %s (%d)" % (where, status_string(status), status))
+        msg = "%s failed: %s (%d)" % (where, status_string(status), status)
+        if status == -3:
+            if cuda is None:
+                f = ctypes.c_char_p()
+                ln = ctypes.c_int(0)
+                code = load().eacb_last_cuda_error(ctypes.byref(f), ctypes.byref(ln))
+                cuda = (code, (f.value or b"").decode(), ln.value)
+            msg += "; cudaError %d at %s:%d" % cuda
+        super().__init__(msg)
 
 
 def load():
@@ -40,6 +48,8 @@ def load():
     sigs = {
         "eacb_version": (ctypes.c_int, []),
         "eacb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+        "eacb_last_cuda_error": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p),
+                                                ctypes.POINTER(ctypes.c_int)]),
         "eacb_workspace_status": (ctypes.c_int, [p, p]),
         "eacb_profile_enable": (None, [ctypes.c_int]),
         "eacb_profile_read": (None, [p, p, p, p]),
@@ -67,6 +77,8 @@ def load():
         "eacb_make_diassoc": (ctypes.c_int, [p, i64, i32, p]),
         "eacb_coassoc_fill": (ctypes.c_int, [p, i32, i32, i32, p, p, p, p, i32, P64, P32, p, sz,
                                              p]),
+        "eacb_batched_workspace_size": (sz, [p, i32, i32]),
+        "eacb_batched_eac": (ctypes.c_int, [p, i32, p, i32, p, sz, p]),
         "eacb_final_clustering_workspace_size": (sz, [i32, i64]),
         "eacb_final_clustering": (ctypes.c_int, [p, p, p, i32, i64, i32, i32, p, P64, P32, p, sz,
                                                  p]),
@@ -77,6 +89,28 @@ def load():
         f.argtypes = args
     _lib = L
     return L
+
+
+class Instance(ctypes.Structure):
+    """struct eacb_instance (include/eacb200.h)."""
+    _fields_ = [("X", ctypes.c_void_p), ("k", ctypes.c_void_p), ("init", ctypes.c_void_p),
+                ("labels", ctypes.c_void_p), ("n", ctypes.c_int32), ("d", ctypes.c_int32),
+                ("P", ctypes.c_int32), ("kmax", ctypes.c_int32), ("n_fclusts", ctypes.c_int64),
+                ("nnz", ctypes.c_int64), ("nnz_discarded", ctypes.c_int64),
+                ("labels_valid", ctypes.c_int32), ("status", ctypes.c_int32),
+                ("ms_ensemble", ctypes.c_float), ("ms_coassoc", ctypes.c_float),
+                ("ms_final", ctypes.c_float), ("worker", ctypes.c_int32),
+                ("cuda_error", ctypes.c_int32), ("cuda_line", ctypes.c_int32)]
+
+
+class BatchOptions(ctypes.Structure):
+    """struct eacb_batch_options (include/eacb200.h)."""
+    _fields_ = [("max_iter", ctypes.c_int32), ("tol", ctypes.c_float),
+                ("label_mode", ctypes.c_int32), ("centroid_mode", ctypes.c_int32),
+                ("cap_mode", ctypes.c_int32), ("max_assocs_factor", ctypes.c_int32),
+                ("n_s", ctypes.c_double), ("n_e", ctypes.c_double), ("val_s", ctypes.c_double),
+                ("val_e", ctypes.c_double), ("n_clusters", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 def extend(sigs):

@@ -15,13 +15,20 @@
 
 #include "../../include/eacb200.h"
 
-#define EACB_CUDA(call)                                   \
-    do {                                                  \
-        cudaError_t _e = (call);                          \
-        if (_e != cudaSuccess) return EACB_ERR_CUDA;      \
+namespace eacb {
+inline void count_launch(int n = 1);
+// the calling thread's last failed CUDA runtime call (eacb_last_cuda_error)
+void note_cuda_error(int code, const char *file, int line);
+}
+#define EACB_CUDA(call)                                           \
+    do {                                                          \
+        cudaError_t _e = (call);                                  \
+        if (_e != cudaSuccess) {                                  \
+            eacb::note_cuda_error((int)_e, __FILE__, __LINE__);   \
+            return EACB_ERR_CUDA;                                 \
+        }                                                         \
     } while (0)
 
-namespace eacb { inline void count_launch(int n = 1); }
 #define EACB_CHECK_LAUNCH()                 \
     do {                                    \
         eacb::count_launch();               \
@@ -83,6 +90,25 @@ struct Carver {
 };
 
 inline cudaStream_t as_stream(uintptr_t s) { return (cudaStream_t)s; }
+
+// Raises a kernel's dynamic shared memory limit to the most the device
+// allows.  Every caller sets the same value, so host threads launching the
+// kernel concurrently with different requests never lower the limit under
+// one another's launch (occupancy follows the request of each launch).
+template <typename F>
+inline cudaError_t allow_max_dyn_smem(F *func)
+{
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, (const void *)func);
+    if (e != cudaSuccess) return e;
+    int dev = 0, optin = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) !=
+        cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute((const void *)func, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - (int)a.sharedSizeBytes);
+}
 
 inline unsigned grid_for(int64_t n, int threads, int64_t max_blocks = 148 * 32)
 {

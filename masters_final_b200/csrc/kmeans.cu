@@ -445,8 +445,7 @@ extern "C" int eacb_kmeans_ensemble(const float *X, int32_t n, int32_t d, int32_
         if ((s = scan_launch<int32_t, int64_t>(w.cnt, w.S, m, 0, &w.S[m], w.scan, st))) return s;
         const size_t place_smem = (size_t)kmax * (sizeof(int64_t) + sizeof(int32_t));
         if (place_smem > 48 * 1024)
-            EACB_CUDA(cudaFuncSetAttribute(k_ml_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)place_smem));
+            EACB_CUDA(allow_max_dyn_smem(k_ml_place));
         k_ml_place<<<(unsigned)(P * nt), 32, place_smem, st>>>(labels, n, kmax, nt, w.S, w.members,
                                                                w.mypos);
         EACB_CHECK_LAUNCH();

@@ -515,8 +515,7 @@ int label_pass_tc(const float *X, int32_t n, int32_t D, int32_t P, const float *
     // at least 100 KB so that no more than two CTAs (2 x 256 TMEM columns)
     // share an SM
     const size_t smem_req = smem < 100 * 1024 ? 100 * 1024 : smem;
-    EACB_CUDA(cudaFuncSetAttribute(k_label_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem_req));
+    EACB_CUDA(allow_max_dyn_smem(k_label_tc));
     dim3 grid((unsigned)(s.n_pad / kTM), (unsigned)P);
     ProfScope ps(PROF_KMEANS, st);
     k_label_tc<<<grid, kTThreads, smem_req, st>>>(X, n, D, s.Kp, C, kk, kmax, s.kt_max, active,

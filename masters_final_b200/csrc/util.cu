@@ -46,7 +46,30 @@ Prof &prof()
     static Prof p = {};
     return p;
 }
+
+struct CudaErrInfo {
+    int code;
+    const char *file;
+    int line;
+};
+static thread_local CudaErrInfo t_cuda_err = {0, nullptr, 0};
+
+void note_cuda_error(int code, const char *file, int line)
+{
+    t_cuda_err.code = code;
+    t_cuda_err.file = file;
+    t_cuda_err.line = line;
+}
 }  // namespace eacb
+
+// The calling thread's last CUDA runtime error seen by the library (0 if
+// none), with the source file and line of the failed call.
+extern "C" int eacb_last_cuda_error(const char **file, int *line)
+{
+    if (file) *file = eacb::t_cuda_err.file ? eacb::t_cuda_err.file : "";
+    if (line) *line = eacb::t_cuda_err.line;
+    return eacb::t_cuda_err.code;
+}
 
 // Profiling: enable/disable and reset counters.
 extern "C" void eacb_profile_enable(int on)

@@ -39,6 +39,23 @@ def gaussian_mixture(n, d, n_centers, seed, sigma=1.0, center_range=10.0,
     return np.ascontiguousarray(x, dtype=np.float32)
 
 
+def batched_instances(m=512, seed=0, n_range=(1000, 50000), dims=(2, 4, 8, 16, 32),
+                      comps=(3, 30), sigma=(0.5, 2.0), center_range=10.0):
+    """The batched EAC workload: ``m`` independent datasets, n log-uniform in
+    ``n_range``, d uniform over ``dims``, a number of Gaussians uniform in
+    [comps[0], comps[1]] with per-component sigma uniform in ``sigma`` and
+    centres uniform in [-center_range, center_range]^d."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(m):
+        n = int(round(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1])))))
+        d = int(rng.choice(dims))
+        c = int(rng.integers(comps[0], comps[1] + 1))
+        out.append(gaussian_mixture(n, d, c, seed=int(rng.integers(1 << 31)), sigma=sigma,
+                                    center_range=center_range))
+    return out
+
+
 def knn_graph(n_vertices, k=16, dim=3, seed=2, wmax=255, wdtype=np.uint8):
     """Symmetric CSR graph of the k nearest neighbours of uniform points in
     [0,1)^dim: every kNN pair becomes one undirected edge (duplicates merged)
