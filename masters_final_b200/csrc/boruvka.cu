@@ -377,147 +377,248 @@ __device__ __forceinline__ uint32_t wbucket(uint32_t w, int wbits)
     return wbits <= 8 ? w : (w >> (wbits - 8));
 }
 
-template <typename WT>
-__global__ void k_whist_csr(const WT *weight, int64_t E, int wbits, unsigned long long *hist)
+// 256-bin histograms.  Weights are heavily skewed (most co-association
+// dissimilarities sit in a few top bins), so a shared atomic per element
+// would serialise on those bins: lanes of a warp holding the same bin combine
+// first (match_any), and every warp owns a private copy of the bins.
+constexpr int kHistThreads = 256;
+
+__device__ __forceinline__ void hist_add(unsigned *h, uint32_t b, bool valid)
 {
-    __shared__ unsigned long long h[256];
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
-    __syncthreads();
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E;
-         e += (int64_t)gridDim.x * blockDim.x)
-        atomicAdd(&h[wbucket(wword(weight[e]), wbits) & 255], 1ull);
-    __syncthreads();
-    for (int i = threadIdx.x; i < 256; i += blockDim.x)
-        if (h[i]) atomicAdd(&hist[i], h[i]);
+    const unsigned act = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    const unsigned peers = __match_any_sync(act, b);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[b], (unsigned)__popc(peers));
 }
 
-__global__ void k_whist_u8(const uint8_t *w, int64_t n, unsigned long long *hist)
+__device__ __forceinline__ void hist_flush(unsigned (*h)[256], unsigned long long *hist)
 {
-    __shared__ unsigned long long h[256];
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
     __syncthreads();
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
-         e += (int64_t)gridDim.x * blockDim.x)
-        atomicAdd(&h[w[e]], 1ull);
-    __syncthreads();
-    for (int i = threadIdx.x; i < 256; i += blockDim.x)
-        if (h[i]) atomicAdd(&hist[i], h[i]);
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kHistThreads / 32; ++w) t += h[w][b];
+        if (t) atomicAdd(&hist[b], t);
+    }
 }
 
-// Edges of a symmetric CSR whose weight bucket is in (lo, hi] and whose
-// endpoints are in different components; one warp per row, each 32-entry
-// chunk reserves its output slots with one atomicAdd (edge order is not
-// deterministic, results are: selection uses a strict total order).
 template <typename WT>
-__global__ void k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest,
-                            const WT *weight, int32_t V, int64_t E, int wbits, int lo, int hi,
-                            const int32_t *label, Pack pk, uint64_t *eout,
-                            unsigned long long *cursor, unsigned long long *best, int *err)
+__global__ void __launch_bounds__(kHistThreads)
+k_whist_csr(const WT *weight, int64_t E, int wbits, unsigned long long *hist)
 {
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    for (int64_t u = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < V;
-         u += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int64_t f = first[u], d = deg[u];
-        if (f < 0 || d < 0 || f + d > E) {
-            if (lane == 0) set_err(err, DEV_BAD_INPUT);
-            continue;
-        }
-        const int32_t lu = label[u];
-        uint64_t m = kNone;
-        for (int64_t e0 = f; e0 < f + d; e0 += 32) {
-            const int64_t e = e0 + lane;
-            bool keep = false;
-            uint64_t k = 0;
-            if (e < f + d) {
-                const int32_t v = dest[e];
-                if (v < 0 || v >= V) {
-                    set_err(err, DEV_BAD_INPUT);
-                } else if (v != (int32_t)u) {
-                    const uint32_t w = wword(weight[e]);
-                    const int b = (int)wbucket(w, wbits);
-                    if (b > lo && b <= hi && label[v] != lu) {
-                        keep = true;
-                        k = pk.make(w, (uint32_t)u, (uint32_t)v);
-                    }
-                }
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, keep);
-            if (!bal) continue;
-            unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(cursor, (unsigned long long)__popc(bal));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (keep) {
-                eout[base + __popc(bal & lt)] = k;
-                m = (k >> 1) < m ? (k >> 1) : m;
-            }
-        }
+    __shared__ unsigned h[kHistThreads / 32][256];
+    for (int i = threadIdx.x; i < (kHistThreads / 32) * 256; i += blockDim.x) (&h[0][0])[i] = 0;
+    __syncthreads();
+    unsigned *mine = h[threadIdx.x >> 5];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    // the loop bound is warp-uniform (match_any needs the whole warp)
+    for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x; e0 < E; e0 += stride) {
+        const int64_t e = e0 + threadIdx.x;
+        const bool ok = e < E;
+        hist_add(mine, ok ? wbucket(wword(weight[e]), wbits) & 255 : 0, ok);
+    }
+    hist_flush(h, hist);
+}
+
+// uint8 weights, 16 per thread per step (128-bit loads)
+__global__ void __launch_bounds__(kHistThreads)
+k_whist_u8(const uint8_t *w, int64_t n, unsigned long long *hist)
+{
+    __shared__ unsigned h[kHistThreads / 32][256];
+    for (int i = threadIdx.x; i < (kHistThreads / 32) * 256; i += blockDim.x) (&h[0][0])[i] = 0;
+    __syncthreads();
+    unsigned *mine = h[threadIdx.x >> 5];
+    int64_t head = (int64_t)((16 - ((uintptr_t)w & 15)) & 15);
+    if (head > n) head = n;
+    const int64_t nv = (n - head) >> 4;               // whole 16-byte vectors
+    const uint4 *v = reinterpret_cast<const uint4 *>(w + head);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q0 = (int64_t)blockIdx.x * blockDim.x; q0 < nv; q0 += stride) {
+        const int64_t q = q0 + threadIdx.x;
+        const bool ok = q < nv;
+        uint4 x = ok ? __ldcs(v + q) : make_uint4(0, 0, 0, 0);
+        const uint32_t wd[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) {
-            const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
-            m = x < m ? x : m;
+        for (int k = 0; k < 16; ++k) hist_add(mine, (wd[k >> 2] >> (8 * (k & 3))) & 255u, ok);
+    }
+    // the unaligned head and the ragged tail, by the first block
+    if (blockIdx.x == 0) {
+        const int64_t tail0 = head + (nv << 4);
+        const int64_t rest = head + (n - tail0);       // < 32 elements
+        const bool ok = (int64_t)threadIdx.x < rest;
+        int64_t e = threadIdx.x < head ? (int64_t)threadIdx.x : tail0 + (threadIdx.x - head);
+        if (threadIdx.x < 32) hist_add(mine, ok ? w[e] : 0u, ok);
+    }
+    hist_flush(h, hist);
+}
+
+// Phase builds: the edges of a weight-bucket range (lo, hi] whose endpoints
+// are in different components, appended to eout, with the first round's
+// minimum-edge selection.  A warp takes a row; the 8 rows of a block reserve
+// their output slots with one atomicAdd per block step (a count pass, then a
+// write pass over the same, now cached, entries), which keeps the shared
+// cursor off the critical path.  Edge order is not deterministic, results
+// are: selection uses a strict total order.
+constexpr int kPhThreads = 256;
+constexpr int kPhWarps = kPhThreads / 32;
+
+// exclusive offsets of the block's per-warp counts in s_cnt, one reservation
+__device__ __forceinline__ void phase_reserve(int64_t *s_cnt, unsigned long long *s_base,
+                                              unsigned long long *cursor, int mult)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t tot = 0;
+        for (int w = 0; w < kPhWarps; ++w) {
+            const int64_t c = s_cnt[w];
+            s_cnt[w] = tot;
+            tot += c;
         }
-        if (lane == 0 && m != kNone) atomicMin(&best[lu], (unsigned long long)m);
+        *s_base = tot ? atomicAdd(cursor, (unsigned long long)(mult * tot)) : 0ull;
+    }
+    __syncthreads();
+}
+
+template <typename WT>
+__global__ void __launch_bounds__(kPhThreads)
+k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const WT *weight,
+            int32_t V, int64_t E, int wbits, int lo, int hi, const int32_t *label, Pack pk,
+            uint64_t *eout, unsigned long long *cursor, unsigned long long *best, int *err)
+{
+    __shared__ int64_t s_cnt[kPhWarps];
+    __shared__ unsigned long long s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int64_t r0 = (int64_t)blockIdx.x * kPhWarps; r0 < V; r0 += (int64_t)gridDim.x * kPhWarps) {
+        const int64_t u = r0 + warp;
+        int64_t f = 0, d = 0;
+        int32_t lu = 0;
+        if (u < V) {
+            f = first[u];
+            d = deg[u];
+            if (f < 0 || d < 0 || f + d > E) {
+                if (lane == 0) set_err(err, DEV_BAD_INPUT);
+                d = 0;
+            } else {
+                lu = label[u];
+            }
+        }
+        auto test = [&](int64_t e, uint32_t &w, int32_t &v) -> bool {
+            if (e >= f + d) return false;
+            v = dest[e];
+            if (v < 0 || v >= V) {
+                set_err(err, DEV_BAD_INPUT);
+                return false;
+            }
+            if (v == (int32_t)u) return false;
+            w = wword(weight[e]);
+            const int b = (int)wbucket(w, wbits);
+            return b > lo && b <= hi && label[v] != lu;
+        };
+        int64_t cnt = 0;
+        for (int64_t e0 = f; e0 < f + d; e0 += 32) {
+            uint32_t w;
+            int32_t v;
+            cnt += __popc(__ballot_sync(0xffffffffu, test(e0 + lane, w, v)));
+        }
+        if (lane == 0) s_cnt[warp] = cnt;
+        phase_reserve(s_cnt, &s_base, cursor, 1);
+        if (cnt) {
+            unsigned long long at = s_base + (unsigned long long)s_cnt[warp];
+            uint64_t m = kNone;
+            for (int64_t e0 = f; e0 < f + d; e0 += 32) {
+                uint32_t w = 0;
+                int32_t v = 0;
+                const bool keep = test(e0 + lane, w, v);
+                const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const uint64_t k = pk.make(w, (uint32_t)u, (uint32_t)v);
+                    eout[at + __popc(bal & lt)] = k;
+                    m = (k >> 1) < m ? (k >> 1) : m;
+                }
+                at += __popc(bal);
+            }
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) {
+                const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
+                m = x < m ? x : m;
+            }
+            if (lane == 0 && m != kNone) atomicMin(&best[lu], (unsigned long long)m);
+        }
+        __syncthreads();          // s_cnt is rewritten by the next step
     }
 }
 
 // Same for an upper-triangle CSR with uint8 weights: both directions of each
 // kept entry.
-__global__ void k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w,
-                              int32_t n, int64_t nnz, int lo, int hi, const int32_t *label,
-                              Pack pk, uint64_t *eout, unsigned long long *cursor,
-                              unsigned long long *best, int *err)
+__global__ void __launch_bounds__(kPhThreads)
+k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, int32_t n,
+              int64_t nnz, int lo, int hi, const int32_t *label, Pack pk, uint64_t *eout,
+              unsigned long long *cursor, unsigned long long *best, int *err)
 {
-    const int lane = threadIdx.x & 31;
+    __shared__ int64_t s_cnt[kPhWarps];
+    __shared__ unsigned long long s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
-         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int64_t s = indptr[i], e_end = indptr[i + 1];
-        if (s < 0 || e_end < s || e_end > nnz) {
-            if (lane == 0) set_err(err, DEV_BAD_INPUT);
-            continue;
+    for (int64_t r0 = (int64_t)blockIdx.x * kPhWarps; r0 < n; r0 += (int64_t)gridDim.x * kPhWarps) {
+        const int64_t i = r0 + warp;
+        int64_t s = 0, e_end = 0;
+        int32_t li = 0;
+        if (i < n) {
+            s = indptr[i];
+            e_end = indptr[i + 1];
+            if (s < 0 || e_end < s || e_end > nnz) {
+                if (lane == 0) set_err(err, DEV_BAD_INPUT);
+                e_end = s;
+            } else {
+                li = label[i];
+            }
         }
-        const int32_t li = label[i];
-        uint64_t m = kNone;
+        auto test = [&](int64_t e, uint32_t &ww, int32_t &j, int32_t &lj) -> bool {
+            if (e >= e_end) return false;
+            j = indices[e];
+            if (j <= i || j >= n) {
+                set_err(err, DEV_BAD_INPUT);
+                return false;
+            }
+            ww = w[e];
+            if ((int)ww <= lo || (int)ww > hi) return false;
+            lj = label[j];
+            return lj != li;
+        };
+        int64_t cnt = 0;
         for (int64_t e0 = s; e0 < e_end; e0 += 32) {
-            const int64_t e = e0 + lane;
-            bool keep = false;
-            uint64_t k = 0;
-            int32_t lj = 0;
-            if (e < e_end) {
-                const int32_t j = indices[e];
-                if (j <= i || j >= n) {
-                    set_err(err, DEV_BAD_INPUT);
-                } else {
-                    const uint32_t ww = w[e];
-                    if ((int)ww > lo && (int)ww <= hi) {
-                        lj = label[j];
-                        if (lj != li) {
-                            keep = true;
-                            k = pk.make(ww, (uint32_t)i, (uint32_t)j);
-                        }
-                    }
+            uint32_t ww;
+            int32_t j, lj;
+            cnt += __popc(__ballot_sync(0xffffffffu, test(e0 + lane, ww, j, lj)));
+        }
+        if (lane == 0) s_cnt[warp] = cnt;
+        phase_reserve(s_cnt, &s_base, cursor, 2);
+        if (cnt) {
+            unsigned long long at = s_base + 2ull * (unsigned long long)s_cnt[warp];
+            uint64_t m = kNone;
+            for (int64_t e0 = s; e0 < e_end; e0 += 32) {
+                uint32_t ww = 0;
+                int32_t j = 0, lj = 0;
+                const bool keep = test(e0 + lane, ww, j, lj);
+                const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const uint64_t k = pk.make(ww, (uint32_t)i, (uint32_t)j);
+                    const unsigned long long p = at + 2ull * __popc(bal & lt);
+                    eout[p] = k;            // i -> j
+                    eout[p + 1] = k | 1ull; // j -> i
+                    m = (k >> 1) < m ? (k >> 1) : m;
+                    atomicMin(&best[lj], (unsigned long long)(k >> 1));
                 }
+                at += 2ull * __popc(bal);
             }
-            const unsigned bal = __ballot_sync(0xffffffffu, keep);
-            if (!bal) continue;
-            unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(cursor, 2ull * __popc(bal));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (keep) {
-                const unsigned long long at = base + 2ull * __popc(bal & lt);
-                eout[at] = k;            // i -> j
-                eout[at + 1] = k | 1ull; // j -> i
-                m = (k >> 1) < m ? (k >> 1) : m;
-                atomicMin(&best[lj], (unsigned long long)(k >> 1));
-            }
-        }
 #pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) {
-            const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
-            m = x < m ? x : m;
+            for (int o = 16; o >= 1; o >>= 1) {
+                const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
+                m = x < m ? x : m;
+            }
+            if (lane == 0 && m != kNone) atomicMin(&best[li], (unsigned long long)m);
         }
-        if (lane == 0 && m != kNone) atomicMin(&best[li], (unsigned long long)m);
+        __syncthreads();
     }
 }
 
@@ -1105,7 +1206,8 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
         // weight phases over the bucket histogram of the entries
         EACB_CUDA(cudaMemsetAsync(g.hist, 0, 256 * sizeof(unsigned long long), st));
         if (E > 0) {
-            k_whist_csr<WT><<<grid_for(E, 256, 148 * 8), 256, 0, st>>>(weight, E, wbits, g.hist);
+            k_whist_csr<WT><<<grid_for(E, kHistThreads, 148 * 8), kHistThreads, 0, st>>>(
+                weight, E, wbits, g.hist);
             EACB_CHECK_LAUNCH();
         }
         auto build = [&](int lo, int hi) -> int {
@@ -1373,7 +1475,8 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
     // 1. minimum spanning forest of the dissimilarity graph, by weight phases
     EACB_CUDA(cudaMemsetAsync(g.hist, 0, 256 * sizeof(unsigned long long), st));
     if (nnz > 0) {
-        k_whist_u8<<<grid_for(nnz, 256, 148 * 8), 256, 0, st>>>(diassoc, nnz, g.hist);
+        k_whist_u8<<<grid_for((nnz + 15) / 16, kHistThreads, 148 * 8), kHistThreads, 0, st>>>(
+            diassoc, nnz, g.hist);
         EACB_CHECK_LAUNCH();
     }
     int64_t n_mst = 0, n_comp = 0;

@@ -200,17 +200,59 @@ __device__ float np_pairwise(const float *a, int64_t n)
     return ret;
 }
 
-// inertia and the convergence test of one iteration (KMeans.py:158-180)
-__global__ void k_inertia(const float *dists, int32_t n, int32_t P, int32_t *active,
-                          float *inertia, int32_t *iters, float tol)
+// inertia and the convergence test of one iteration (KMeans.py:158-180).
+// One block per partition.  The top levels of numpy's split tree are
+// expanded while every node is still split (longer than 128) and there are
+// at most kInertiaThreads nodes; each thread sums one node's subtree with the
+// sequential walk, then the expanded levels are added back pairwise in the
+// tree's own order, so the result is bit-identical to the sequential sum.
+constexpr int kInertiaThreads = 256;
+__global__ void __launch_bounds__(kInertiaThreads)
+k_inertia(const float *dists, int32_t n, int32_t P, int32_t *active, float *inertia,
+          int32_t *iters, float tol)
 {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= P || !active[p]) return;
-    const float I = np_pairwise(dists + (int64_t)p * n, n);
-    const float err = fabsf(__fsub_rn(I, inertia[p]));
-    inertia[p] = I;
-    iters[p] += 1;
-    if (err <= tol) active[p] = 0;
+    __shared__ int64_t s_off[kInertiaThreads], s_len[kInertiaThreads];
+    __shared__ float s_val[kInertiaThreads];
+    __shared__ int s_cnt;
+    const int p = blockIdx.x;
+    if (p >= P || !active[p]) return;          // uniform across the block
+    const float *a = dists + (int64_t)p * n;
+    if (threadIdx.x == 0) {
+        s_off[0] = 0;
+        s_len[0] = n;
+        int cnt = 1;
+        while (cnt * 2 <= kInertiaThreads) {
+            bool split_all = true;
+            for (int q = 0; q < cnt; ++q)
+                if (s_len[q] <= 128) split_all = false;
+            if (!split_all) break;
+            // children of node q go to 2q and 2q+1 (back to front, in place)
+            for (int q = cnt - 1; q >= 0; --q) {
+                const int64_t o = s_off[q], l = s_len[q];
+                int64_t n2 = l / 2;
+                n2 -= n2 % 8;
+                s_off[2 * q] = o;
+                s_len[2 * q] = n2;
+                s_off[2 * q + 1] = o + n2;
+                s_len[2 * q + 1] = l - n2;
+            }
+            cnt *= 2;
+        }
+        s_cnt = cnt;
+    }
+    __syncthreads();
+    const int cnt = s_cnt;
+    if ((int)threadIdx.x < cnt) s_val[threadIdx.x] = np_pairwise(a + s_off[threadIdx.x], s_len[threadIdx.x]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int c = cnt; c > 1; c >>= 1)
+            for (int q = 0; q < c / 2; ++q) s_val[q] = __fadd_rn(s_val[2 * q], s_val[2 * q + 1]);
+        const float I = s_val[0];
+        const float err = fabsf(__fsub_rn(I, inertia[p]));
+        inertia[p] = I;
+        iters[p] += 1;
+        if (err <= tol) active[p] = 0;
+    }
 }
 
 // float32 (reference) or float64 sums of each cluster's members in point order
@@ -435,7 +477,8 @@ extern "C" int eacb_kmeans_ensemble(const float *X, int32_t n, int32_t d, int32_
             s = label_pass_f32(X, n, d, P, centroids, k, kmax, w.active, labels, w.dists, w.amb,
                                w.namb, st);
         if (s) return s;
-        k_inertia<<<(P + 127) / 128, 128, 0, st>>>(w.dists, n, P, w.active, w.inertia, w.iters, tol);
+        k_inertia<<<P, kInertiaThreads, 0, st>>>(w.dists, n, P, w.active, w.inertia, w.iters,
+                                                  tol);
         EACB_CHECK_LAUNCH();
         if (it + 1 >= max_iter) break;
         // centroids of the partitions still running

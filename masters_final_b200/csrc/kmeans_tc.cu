@@ -495,9 +495,6 @@ int label_pass_tc(const float *X, int32_t n, int32_t D, int32_t P, const float *
     k_prep_centroids<<<grid_for((int64_t)P * s.kt_max * kTN, 128), 128, 0, st>>>(
         C, kk, kmax, P, D, s.Kp, s.kt_max, s.mu, active, s.B, s.nc, s.cmax2);
     EACB_CHECK_LAUNCH();
-    // error model of the screened distance, doubled for margin: BF16 split
-    // (3 * 2^-16), FP32 accumulation over 3D products (3D * 2^-23), the
-    // norms and the epilogue arithmetic ((D + 6) * 2^-24)
     // Error model of the screened distance, doubled for margin.  The dot
     // product: the three-way split drops < 3 * 2^-24 |x||c|; the MMA adds
     // the h*h group last, so its accumulation error is at most
