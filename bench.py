@@ -288,6 +288,10 @@ def run_ours(args):
            "h2d_bytes_per_step": int(dest.nbytes + w.nbytes + first.nbytes + deg.nbytes),
            "d2h_bytes_per_step": int(4 * (V - 1))}
 
+    sharded = None
+    if world > 1 and not args.no_eac:
+        sharded = eac_batched_sharded_measurement(torch, dist, world)
+
     if rank == 0:
         peak, peak_kind = measured_peak()
         achieved = (pbytes[0] / (pms[0] / 1000.0)) / 1e9 if pms[0] > 0 else None
@@ -309,6 +313,8 @@ def run_ours(args):
             line["cpu_baseline"] = cpu_baseline(indptr, dest, w, n_edges)
         if world == 1 and not args.no_eac:
             line["eac"] = eac_measurements(args)
+        if sharded is not None:
+            line["eac_batched_sharded"] = sharded
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -323,7 +329,14 @@ EAC_WORKLOADS = {
                             cr=10.0, sigma=1.0, seed=0),
     "eac_500k_16d_200p": dict(n=500_000, d=16, comps=50, P=200, k=(350, 711), aniso=True,
                               cr=20.0, sigma=1.0, seed=3),
+    "eac_2m_8d_100p": dict(n=2_000_000, d=8, comps=200, P=100, k=(700, 1401), aniso=False,
+                           cr=50.0, sigma=(0.5, 3.0), seed=5),
 }
+# many independent datasets in one batched call (EAC.batched.eac_batch): n
+# log-uniform in [1000, 50000], d in {2,4,8,16,32}, 3-30 Gaussians with
+# sigma U[0.5, 2], centres U[-10, 10]^d, 50 partitions, k range
+# [ceil(sqrt(n)/2), ceil(sqrt(n))) per dataset
+EAC_BATCHED = dict(instances=512, P=50, seed=0, workers=32)
 
 
 def eac_run_once(X, cfg, mode, torch):
@@ -364,11 +377,21 @@ def eac_measurements(args):
         warm, steps = (3, 5) if small else (1, 1)
         res = {}
         parts = {}
+        e = None
+        def release():
+            # large workloads: the previous matrix goes before the next one is
+            # built (small ones keep the allocator's cache, as a user would)
+            if not small:
+                torch.cuda.empty_cache()
         for mode in ("bf16", "cuda"):
             for _ in range(warm):
+                e = None
+                release()
                 eac_run_once(X, cfg, mode, torch)
             tot = [0.0, 0.0, 0.0]
             for _ in range(steps):
+                e = None
+                release()
                 flush.fill_(1)
                 ms, labels, e = eac_run_once(X, cfg, mode, torch)
                 tot = [a + b for a, b in zip(tot, ms)]
@@ -384,7 +407,63 @@ def eac_measurements(args):
         res["n_fclusts"] = int(e.n_fclusts)
         res["config"] = {k: (list(v) if isinstance(v, tuple) else v) for k, v in cfg.items()}
         out[name] = res
+        del X, e
+        torch.cuda.empty_cache()
+    out["eac_batched_512"] = eac_batched_measurement(torch)
     return out
+
+
+def eac_batched_sharded_measurement(torch, dist, world):
+    """The batched workload split across the ranks (instances balanced by
+    cost, one exchange of results at the end): Σn / max-over-ranks time of
+    one eac_batch_distributed call, after one warm-up call."""
+    from masters_final_b200 import workloads as W
+    from masters_final_b200.EAC.batched import eac_batch_distributed
+    cfg = EAC_BATCHED
+    xs = W.batched_instances(cfg["instances"], seed=cfg["seed"])
+    N = int(sum(x.shape[0] for x in xs))
+    eac_batch_distributed(xs, cfg["P"], n_workers=cfg["workers"])
+    dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = eac_batch_distributed(xs, cfg["P"], n_workers=cfg["workers"])
+    torch.cuda.synchronize()
+    t = torch.tensor([time.perf_counter() - t0], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dt = float(t.item())
+    return {"points_per_s": N / dt, "s": dt, "sum_n": N, "instances": len(xs),
+            "n_gpus": world, "scaling": "strong", "failed": int(sum(r.status != 0 for r in out)),
+            "timing": "host wall clock around the call, max over ranks (the call ends with "
+                      "an exchange of results)",
+            "config": {**cfg, "label_mode": "bf16"}}
+
+
+def eac_batched_measurement(torch):
+    """Batched EAC points/s (sum of n over all datasets / wall time of one
+    eac_batch call, data on the device), after one warm-up call."""
+    from masters_final_b200 import workloads as W
+    from masters_final_b200.EAC.batched import eac_batch, draw_instance_params, k_range_rule1
+    cfg = EAC_BATCHED
+    xs = W.batched_instances(cfg["instances"], seed=cfg["seed"])
+    ps = [draw_instance_params(x.shape[0], k_range_rule1(x.shape[0]), cfg["P"], i)
+          for i, x in enumerate(xs)]
+    Xd = [torch.from_numpy(x).cuda() for x in xs]
+    N = int(sum(x.shape[0] for x in xs))
+    eac_batch(Xd, params=ps, n_workers=cfg["workers"], return_device=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = eac_batch(Xd, params=ps, n_workers=cfg["workers"], return_device=True)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    st = np.array([a.ms_stages for a in r])
+    return {"points_per_s": N / dt, "s": dt, "sum_n": N, "instances": len(xs),
+            "nnz_total": int(sum(a.nnz for a in r)),
+            "nnz_discarded_total": int(sum(a.nnz_discarded for a in r)),
+            "failed": int(sum(a.status != 0 for a in r)),
+            "worker_ms_sums": {"ensemble": float(st[:, 0].sum()), "coassoc": float(st[:, 1].sum()),
+                               "final": float(st[:, 2].sum())},
+            "config": {**cfg, "n_range": [1000, 50000], "d": [2, 4, 8, 16, 32],
+                       "gaussians": [3, 30], "sigma": [0.5, 2.0], "label_mode": "bf16"}}
 
 
 def main():

@@ -132,3 +132,68 @@ def eac_batch(datasets, n_partitions=50, k_ranges=None, seeds=None, iters=3, tol
         err.results = out
         raise err
     return out
+
+
+def instance_cost(n, d, P, kmax):
+    """Relative GPU cost of one instance: co-association visits ~ P n (n / k)
+    plus the ensemble's P n k d distance work."""
+    k = max(int(kmax), 1)
+    return float(P) * n * (n / k) + float(P) * n * k * d / 64.0
+
+
+def shard_instances(costs, world):
+    """Deterministic longest-processing-time assignment of instances to
+    `world` ranks: returns one ascending index list per rank."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    out = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        out[r].append(i)
+        load[r] += costs[i]
+    return [sorted(o) for o in out]
+
+
+def eac_batch_distributed(datasets, n_partitions=50, k_ranges=None, seeds=None, group=None,
+                          runner=None, **kw):
+    """eac_batch over the ranks of a torch.distributed process group: every
+    rank receives the whole dataset list, runs its share (balanced by
+    instance_cost, no data-path collective) on its own GPU, and the results
+    are exchanged once at the end (all_gather_object), so every rank returns
+    the full list in input order.  The host draws of instance i use seed
+    seeds[i] (default i) whichever rank runs it, so results equal a
+    single-GPU call."""
+    import torch.distributed as dist
+    run = runner or eac_batch
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    m = len(datasets)
+    ns = [int(x.shape[0]) for x in datasets]
+    kr = [k_ranges[i] if k_ranges is not None else k_range_rule1(ns[i]) for i in range(m)]
+    sd = [seeds[i] if seeds is not None else i for i in range(m)]
+    costs = [instance_cost(ns[i], int(datasets[i].shape[1]), n_partitions, kr[i][1])
+             for i in range(m)]
+    mine = shard_instances(costs, world)[rank]
+    params = [draw_instance_params(ns[i], kr[i], n_partitions, sd[i]) for i in mine]
+    kw["return_device"] = False              # results travel between ranks as numpy
+    status = 0
+    res = []
+    if mine:
+        try:
+            res = run([datasets[i] for i in mine], n_partitions=n_partitions, params=params, **kw)
+        except _lib.EACBError as e:          # every rank still joins the exchange
+            status = e.status
+            res = getattr(e, "results", [])
+    local = (status, [(i, r) for i, r in zip(mine, res)])
+    gathered = [None] * world
+    dist.all_gather_object(gathered, local, group=group)
+    out = [None] * m
+    first_err = 0
+    for st, part in gathered:
+        first_err = first_err or st
+        for i, r in part:
+            out[i] = r
+    if first_err:
+        err = _lib.EACBError(first_err, "distributed batched eac", (0, "batched instance", 0))
+        err.results = out
+        raise err
+    return out

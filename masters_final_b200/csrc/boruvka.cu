@@ -88,6 +88,15 @@ __device__ __forceinline__ uint32_t wword(float x)
 
 constexpr uint64_t kNone = ~0ull;
 
+// atomicMin that is skipped when the candidate cannot lower the slot.  Within
+// a kernel the slots only decrease, so a (possibly older) L2 value that the
+// candidate does not beat means the atomic would change nothing; late
+// rounds, whose few supervertices receive most edges, then issue few atomics.
+__device__ __forceinline__ void min_if_lower(unsigned long long *slot, uint64_t v)
+{
+    if (v < __ldcg(slot)) atomicMin(slot, (unsigned long long)v);
+}
+
 // One atomicMin per run of equal `su` among consecutive lanes.
 __device__ __forceinline__ void seg_min_atomic(bool valid, int32_t su, uint64_t sel,
                                                unsigned long long *best)
@@ -106,7 +115,7 @@ __device__ __forceinline__ void seg_min_atomic(bool valid, int32_t su, uint64_t 
     }
     int32_t next = __shfl_down_sync(0xffffffffu, key, 1);
     bool tail = (lane == 31) || (next != key);
-    if (valid && tail) atomicMin(&best[su], (unsigned long long)m);
+    if (valid && tail) min_if_lower(&best[su], m);
 }
 
 constexpr int kET = 256;   // edge-tile threads
@@ -461,10 +470,15 @@ k_whist_u8(const uint8_t *w, int64_t n, unsigned long long *hist)
 constexpr int kPhThreads = 256;
 constexpr int kPhWarps = kPhThreads / 32;
 
-// exclusive offsets of the block's per-warp counts in s_cnt, one reservation
-__device__ __forceinline__ void phase_reserve(int64_t *s_cnt, unsigned long long *s_base,
-                                              unsigned long long *cursor, int mult)
+// Exclusive offsets of the block's per-warp counts in s_cnt and one
+// reservation of mult * total slots.  A reservation that would pass `cap`
+// (the output capacity) writes nothing and raises DEV_CAPACITY; it returns
+// false to every thread of the block.
+__device__ __forceinline__ bool phase_reserve(int64_t *s_cnt, unsigned long long *s_base,
+                                              unsigned long long *cursor, int mult,
+                                              unsigned long long cap, int *err)
 {
+    __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int64_t tot = 0;
@@ -473,76 +487,100 @@ __device__ __forceinline__ void phase_reserve(int64_t *s_cnt, unsigned long long
             s_cnt[w] = tot;
             tot += c;
         }
-        *s_base = tot ? atomicAdd(cursor, (unsigned long long)(mult * tot)) : 0ull;
+        const unsigned long long need = (unsigned long long)(mult * tot);
+        const unsigned long long b = tot ? atomicAdd(cursor, need) : 0ull;
+        *s_base = b;
+        s_ok = b + need <= cap;
+        if (!s_ok) set_err(err, DEV_CAPACITY);
     }
     __syncthreads();
+    return s_ok != 0;
 }
 
 template <typename WT>
 __global__ void __launch_bounds__(kPhThreads)
 k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const WT *weight,
             int32_t V, int64_t E, int wbits, int lo, int hi, const int32_t *label, Pack pk,
-            uint64_t *eout, unsigned long long *cursor, unsigned long long *best, int *err)
+            uint64_t *eout, unsigned long long *cursor, unsigned long long cap,
+            unsigned long long *best, int *err)
 {
+    // rows are short (graph degrees): a warp takes kPhRows consecutive rows
+    // per block step, so one reservation covers 8 * kPhRows rows
+    constexpr int kPhRows = 16;
     __shared__ int64_t s_cnt[kPhWarps];
     __shared__ unsigned long long s_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    for (int64_t r0 = (int64_t)blockIdx.x * kPhWarps; r0 < V; r0 += (int64_t)gridDim.x * kPhWarps) {
-        const int64_t u = r0 + warp;
-        int64_t f = 0, d = 0;
-        int32_t lu = 0;
-        if (u < V) {
-            f = first[u];
-            d = deg[u];
-            if (f < 0 || d < 0 || f + d > E) {
-                if (lane == 0) set_err(err, DEV_BAD_INPUT);
-                d = 0;
-            } else {
-                lu = label[u];
-            }
+    auto test = [&](int64_t u, int64_t f, int64_t d, int32_t lu, int64_t e, uint32_t &w,
+                    int32_t &v) -> bool {
+        if (e >= f + d) return false;
+        v = dest[e];
+        if (v < 0 || v >= V) {
+            set_err(err, DEV_BAD_INPUT);
+            return false;
         }
-        auto test = [&](int64_t e, uint32_t &w, int32_t &v) -> bool {
-            if (e >= f + d) return false;
-            v = dest[e];
-            if (v < 0 || v >= V) {
-                set_err(err, DEV_BAD_INPUT);
-                return false;
-            }
-            if (v == (int32_t)u) return false;
-            w = wword(weight[e]);
-            const int b = (int)wbucket(w, wbits);
-            return b > lo && b <= hi && label[v] != lu;
-        };
+        if (v == (int32_t)u) return false;
+        w = wword(weight[e]);
+        const int b = (int)wbucket(w, wbits);
+        return b > lo && b <= hi && label[v] != lu;
+    };
+    auto row = [&](int64_t u, int64_t &f, int64_t &d, int32_t &lu) {
+        f = 0;
+        d = 0;
+        lu = 0;
+        if (u >= V) return;
+        f = first[u];
+        d = deg[u];
+        if (f < 0 || d < 0 || f + d > E) {
+            if (lane == 0) set_err(err, DEV_BAD_INPUT);
+            d = 0;
+            return;
+        }
+        lu = label[u];
+    };
+    const int64_t step = (int64_t)kPhWarps * kPhRows;
+    for (int64_t r0 = (int64_t)blockIdx.x * step; r0 < V; r0 += (int64_t)gridDim.x * step) {
+        const int64_t u0 = r0 + (int64_t)warp * kPhRows;
         int64_t cnt = 0;
-        for (int64_t e0 = f; e0 < f + d; e0 += 32) {
-            uint32_t w;
-            int32_t v;
-            cnt += __popc(__ballot_sync(0xffffffffu, test(e0 + lane, w, v)));
+        for (int r = 0; r < kPhRows; ++r) {
+            int64_t f, d;
+            int32_t lu;
+            row(u0 + r, f, d, lu);
+            for (int64_t e0 = f; e0 < f + d; e0 += 32) {
+                uint32_t w;
+                int32_t v;
+                cnt += __popc(__ballot_sync(0xffffffffu, test(u0 + r, f, d, lu, e0 + lane, w, v)));
+            }
         }
         if (lane == 0) s_cnt[warp] = cnt;
-        phase_reserve(s_cnt, &s_base, cursor, 1);
-        if (cnt) {
+        const bool fits = phase_reserve(s_cnt, &s_base, cursor, 1, cap, err);
+        if (cnt && fits) {
             unsigned long long at = s_base + (unsigned long long)s_cnt[warp];
-            uint64_t m = kNone;
-            for (int64_t e0 = f; e0 < f + d; e0 += 32) {
-                uint32_t w = 0;
-                int32_t v = 0;
-                const bool keep = test(e0 + lane, w, v);
-                const unsigned bal = __ballot_sync(0xffffffffu, keep);
-                if (keep) {
-                    const uint64_t k = pk.make(w, (uint32_t)u, (uint32_t)v);
-                    eout[at + __popc(bal & lt)] = k;
-                    m = (k >> 1) < m ? (k >> 1) : m;
+            for (int r = 0; r < kPhRows; ++r) {
+                const int64_t u = u0 + r;
+                int64_t f, d;
+                int32_t lu;
+                row(u, f, d, lu);
+                uint64_t m = kNone;
+                for (int64_t e0 = f; e0 < f + d; e0 += 32) {
+                    uint32_t w = 0;
+                    int32_t v = 0;
+                    const bool keep = test(u, f, d, lu, e0 + lane, w, v);
+                    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                    if (keep) {
+                        const uint64_t k = pk.make(w, (uint32_t)u, (uint32_t)v);
+                        eout[at + __popc(bal & lt)] = k;
+                        m = (k >> 1) < m ? (k >> 1) : m;
+                    }
+                    at += __popc(bal);
                 }
-                at += __popc(bal);
-            }
 #pragma unroll
-            for (int o = 16; o >= 1; o >>= 1) {
-                const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
-                m = x < m ? x : m;
+                for (int o = 16; o >= 1; o >>= 1) {
+                    const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
+                    m = x < m ? x : m;
+                }
+                if (lane == 0 && m != kNone) min_if_lower(&best[lu], m);
             }
-            if (lane == 0 && m != kNone) atomicMin(&best[lu], (unsigned long long)m);
         }
         __syncthreads();          // s_cnt is rewritten by the next step
     }
@@ -552,18 +590,20 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
 // kept entry.
 __global__ void __launch_bounds__(kPhThreads)
 k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, int32_t n,
-              int64_t nnz, int lo, int hi, const int32_t *label, Pack pk, uint64_t *eout,
-              unsigned long long *cursor, unsigned long long *best, int *err)
+              int64_t nnz, int lo, int hi, int64_t row0, int64_t row1, const int32_t *label,
+              Pack pk, uint64_t *eout, unsigned long long *cursor, unsigned long long cap,
+              unsigned long long *best, int *err)
 {
     __shared__ int64_t s_cnt[kPhWarps];
     __shared__ unsigned long long s_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    for (int64_t r0 = (int64_t)blockIdx.x * kPhWarps; r0 < n; r0 += (int64_t)gridDim.x * kPhWarps) {
+    for (int64_t r0 = row0 + (int64_t)blockIdx.x * kPhWarps; r0 < row1;
+         r0 += (int64_t)gridDim.x * kPhWarps) {
         const int64_t i = r0 + warp;
         int64_t s = 0, e_end = 0;
         int32_t li = 0;
-        if (i < n) {
+        if (i < row1) {
             s = indptr[i];
             e_end = indptr[i + 1];
             if (s < 0 || e_end < s || e_end > nnz) {
@@ -592,8 +632,8 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
             cnt += __popc(__ballot_sync(0xffffffffu, test(e0 + lane, ww, j, lj)));
         }
         if (lane == 0) s_cnt[warp] = cnt;
-        phase_reserve(s_cnt, &s_base, cursor, 2);
-        if (cnt) {
+        const bool fits = phase_reserve(s_cnt, &s_base, cursor, 2, cap, err);
+        if (cnt && fits) {
             unsigned long long at = s_base + 2ull * (unsigned long long)s_cnt[warp];
             uint64_t m = kNone;
             for (int64_t e0 = s; e0 < e_end; e0 += 32) {
@@ -602,12 +642,14 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
                 const bool keep = test(e0 + lane, ww, j, lj);
                 const unsigned bal = __ballot_sync(0xffffffffu, keep);
                 if (keep) {
+                    // the chunk's i -> j words, then its j -> i words: runs of
+                    // equal source for the min-edge selection of later rounds
                     const uint64_t k = pk.make(ww, (uint32_t)i, (uint32_t)j);
-                    const unsigned long long p = at + 2ull * __popc(bal & lt);
-                    eout[p] = k;            // i -> j
-                    eout[p + 1] = k | 1ull; // j -> i
+                    const unsigned long long p = at + __popc(bal & lt);
+                    eout[p] = k;
+                    eout[p + __popc(bal)] = k | 1ull;
                     m = (k >> 1) < m ? (k >> 1) : m;
-                    atomicMin(&best[lj], (unsigned long long)(k >> 1));
+                    min_if_lower(&best[lj], k >> 1);
                 }
                 at += 2ull * __popc(bal);
             }
@@ -616,11 +658,17 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
                 const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
                 m = x < m ? x : m;
             }
-            if (lane == 0 && m != kNone) atomicMin(&best[li], (unsigned long long)m);
+            if (lane == 0 && m != kNone) min_if_lower(&best[li], m);
         }
         __syncthreads();
     }
 }
+
+// One phase: the entries with weight bucket in (lo, hi] of rows [r0, r1).
+struct Phase {
+    int lo, hi;
+    int64_t r0, r1;
+};
 
 // Phase ranges (lo, hi] of weight buckets: cut the bucket histogram at the
 // given cumulative fractions of the entries.
@@ -891,21 +939,24 @@ struct Engine {
     // MST by weight phases (see k_phase_csr).  `hist` must hold the 256-bucket
     // weight histogram; build(lo, hi) launches one phase's edge build into ea
     // (slots reserved through cnt[C_CURSOR]) with its selection into best.
-    template <typename Build>
-    int run_phased(Pack pk, Build build, cudaStream_t st, int64_t *n_mst_out, int64_t *n_comp_out)
+    int read_hist(cudaStream_t st, unsigned long long h[256])
     {
-        unsigned long long h[256];
-        EACB_CUDA(cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, st));
+        EACB_CUDA(cudaMemcpyAsync(h, hist, 256 * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, st));
         EACB_CUDA(cudaStreamSynchronize(st));
-        const double fracs[3] = {0.125, 0.5, 1.0};
-        int lo[8], hi[8];
-        const int np = phase_ranges(h, fracs, 3, lo, hi);
+        return EACB_OK;
+    }
+
+    template <typename Build>
+    int run_phased(Pack pk, const std::vector<Phase> &plan, Build build, cudaStream_t st,
+                   int64_t *n_mst_out, int64_t *n_comp_out)
+    {
         int32_t V = V0;
         mst_base = 0;
-        for (int q = 0; q < np; ++q) {
+        for (const Phase &ph : plan) {
             EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V, st));
             EACB_CUDA(cudaMemsetAsync(&cnt[C_CURSOR], 0, sizeof(int64_t), st));
-            int s = build(lo[q], hi[q]);
+            int s = build(ph);
             if (s) return s;
             int64_t Ep = 0;
             int e = 0;
@@ -1206,19 +1257,32 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
         // weight phases over the bucket histogram of the entries
         EACB_CUDA(cudaMemsetAsync(g.hist, 0, 256 * sizeof(unsigned long long), st));
         if (E > 0) {
-            k_whist_csr<WT><<<grid_for(E, kHistThreads, 148 * 8), kHistThreads, 0, st>>>(
-                weight, E, wbits, g.hist);
+            if (sizeof(WT) == 1)
+                k_whist_u8<<<grid_for((E + 15) / 16, kHistThreads, 148 * 8), kHistThreads, 0,
+                             st>>>((const uint8_t *)weight, E, g.hist);
+            else
+                k_whist_csr<WT><<<grid_for(E, kHistThreads, 148 * 8), kHistThreads, 0, st>>>(
+                    weight, E, wbits, g.hist);
             EACB_CHECK_LAUNCH();
         }
-        auto build = [&](int lo, int hi) -> int {
+        unsigned long long h[256];
+        if ((s = g.read_hist(st, h))) return s;
+        const double fracs[3] = {0.125, 0.5, 1.0};
+        int lo[8], hi[8];
+        const int np = phase_ranges(h, fracs, 3, lo, hi);
+        std::vector<Phase> plan;
+        for (int q = 0; q < np; ++q) plan.push_back(Phase{lo[q], hi[q], 0, V});
+        // a phase holds a subset of the E entries: the edge array always fits
+        auto build = [&](const Phase &ph) -> int {
             if (E == 0) return EACB_OK;
-            k_phase_csr<WT><<<gr, 256, 0, st>>>(first, deg, dest, weight, V, E, wbits, lo, hi,
-                                                g.label, pk, g.ea,
-                                                (unsigned long long *)&g.cnt[C_CURSOR], g.best, g.err);
+            k_phase_csr<WT><<<gr, kPhThreads, 0, st>>>(
+                first, deg, dest, weight, V, E, wbits, ph.lo, ph.hi, g.label, pk, g.ea,
+                (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best,
+                g.err);
             EACB_CHECK_LAUNCH();
             return EACB_OK;
         };
-        if ((s = g.run_phased(pk, build, st, &n_mst, &n_comp))) return s;
+        if ((s = g.run_phased(pk, plan, build, st, &n_mst, &n_comp))) return s;
     } else {
         if (E > 0) {
             // dead words everywhere first: entries outside every row, self loops
@@ -1430,11 +1494,71 @@ extern "C" int eacb_connected_components(const int32_t *dest, const void *weight
                         n_edges, nullptr, &dummy, labels, host_n_comps, ws, ws_bytes, stream);
 }
 
+// Edge-array capacity of the final clustering (directed words).  A phase
+// never holds more than half the entries (both directions: nnz words), and
+// at least 8 n + 2^20 words (every row fits, and the forest's 2 (n - 1)),
+// so the workspace stays near 8 bytes per entry instead of 16.
+static int64_t final_edge_cap(int32_t n, int64_t nnz)
+{
+    const int64_t lo = 8 * (int64_t)n + (1 << 20);
+    const int64_t want = nnz > lo ? nnz : lo;
+    const int64_t all = 2 * nnz > 2 * (int64_t)n ? 2 * nnz : 2 * (int64_t)n;
+    return want < all ? want : all;
+}
+
+// Phases of the final clustering: the weight ranges of the cumulative
+// fractions (0.125, 0.5, 1), each cut further so that its entries fit the
+// edge array (cap_entries upper entries, i.e. 2 cap_entries words); a single
+// weight with more entries than that is split by row ranges (the order
+// (w, a, b) keeps a row range of one weight contiguous).
+static int plan_final_phases(const unsigned long long h[256], int64_t cap_entries,
+                             const int64_t *d_indptr, int32_t n, cudaStream_t st,
+                             std::vector<Phase> &plan)
+{
+    const double fracs[3] = {0.125, 0.5, 1.0};
+    int lo[8], hi[8];
+    const int np = phase_ranges(h, fracs, 3, lo, hi);
+    std::vector<int64_t> ip;     // host row pointers, fetched only if a weight needs splitting
+    for (int q = 0; q < np; ++q) {
+        int start = lo[q];        // current range is (start, b]
+        unsigned long long acc = 0;
+        for (int b = lo[q] + 1; b <= hi[q]; ++b) {
+            if (acc + h[b] <= (unsigned long long)cap_entries) {
+                acc += h[b];
+                continue;
+            }
+            if (acc) plan.push_back(Phase{start, b - 1, 0, n});
+            start = b - 1;
+            acc = 0;
+            if (h[b] <= (unsigned long long)cap_entries) {
+                acc = h[b];
+                continue;
+            }
+            // weight b alone: rows in pieces of at most cap_entries entries
+            if (ip.empty()) {
+                ip.resize((size_t)n + 1);
+                EACB_CUDA(cudaMemcpyAsync(ip.data(), d_indptr, sizeof(int64_t) * ((size_t)n + 1),
+                                          cudaMemcpyDeviceToHost, st));
+                EACB_CUDA(cudaStreamSynchronize(st));
+            }
+            int64_t r0 = 0;
+            while (r0 < n) {
+                int64_t r1 = r0 + 1;
+                while (r1 < n && ip[r1 + 1] - ip[r0] <= cap_entries) ++r1;
+                plan.push_back(Phase{b - 1, b, r0, r1});
+                r0 = r1;
+            }
+            start = b;
+        }
+        if (acc) plan.push_back(Phase{start, hi[q], 0, n});
+    }
+    return EACB_OK;
+}
+
 static void carve_final(Carver &c, int32_t n, int64_t nnz, Engine *g, int64_t **hist,
                         CutPlan **plan, int32_t **cmin)
 {
-    int64_t emax = 2 * nnz > 2 * (int64_t)n ? 2 * nnz : 2 * (int64_t)n;
-    *g = Engine::carve(c, n, emax);
+    *g = Engine::carve(c, n, final_edge_cap(n, nnz));
     *hist = c.take<int64_t>(256);
     *plan = c.take<CutPlan>(1);
     *cmin = c.take<int32_t>(n);
@@ -1480,15 +1604,19 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
         EACB_CHECK_LAUNCH();
     }
     int64_t n_mst = 0, n_comp = 0;
-    auto build = [&](int lo, int hi) -> int {
+    unsigned long long wh[256];
+    if ((s = g.read_hist(st, wh))) return s;
+    std::vector<Phase> phases;
+    if ((s = plan_final_phases(wh, g.Emax / 2, indptr, n, st, phases))) return s;
+    auto build = [&](const Phase &ph) -> int {
         if (nnz == 0) return EACB_OK;
-        k_phase_upper<<<grid_for((int64_t)n * 32, 256), 256, 0, st>>>(
-            indptr, indices, diassoc, n, nnz, lo, hi, g.label, pk, g.ea,
-            (unsigned long long *)&g.cnt[C_CURSOR], g.best, g.err);
+        k_phase_upper<<<grid_for((ph.r1 - ph.r0) * 32, kPhThreads), kPhThreads, 0, st>>>(
+            indptr, indices, diassoc, n, nnz, ph.lo, ph.hi, ph.r0, ph.r1, g.label, pk, g.ea,
+            (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best, g.err);
         EACB_CHECK_LAUNCH();
         return EACB_OK;
     };
-    if ((s = g.run_phased(pk, build, st, &n_mst, &n_comp))) return s;
+    if ((s = g.run_phased(pk, phases, build, st, &n_mst, &n_comp))) return s;
     // 2. lifetime rule on the weight histogram
     EACB_CUDA(cudaMemsetAsync(hist, 0, 256 * sizeof(int64_t), st));
     if (n_mst > 0) {

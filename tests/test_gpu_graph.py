@@ -191,3 +191,30 @@ def test_final_clustering_disconnected(T):
         nc2, lab2 = oracle.sp_sl_lifetime(n, a, b, w, P)
         assert nc == nc2
         assert np.array_equal(labels, lab2)
+
+
+def test_final_clustering_capacity_split_phases(T):
+    """More entries than the final clustering's edge array holds at once, with
+    one weight owning most of them: the weight is processed in row-range
+    phases (the forest and the labels must not change)."""
+    from masters_final_b200 import _lib
+    from masters_final_b200.EAC.eac import sp_sl_lifetime_csr
+    rng = np.random.default_rng(8)
+    n = 12_000
+    m = 2_600_000                                   # > 8 n + 2^20 upper entries
+    a = rng.integers(0, n - 1, m)
+    b = a + 1 + (rng.random(m) * (n - 1 - a)).astype(np.int64)
+    key = np.unique(a * n + b)
+    a, b = key // n, key % n
+    w = rng.integers(1, 60, a.size).astype(np.uint8)
+    w[rng.random(a.size) < 0.7] = 45                # one weight holds ~70% of the entries
+    indptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(a, minlength=n), out=indptr[1:])
+    L = _lib.load()
+    assert L.eacb_final_clustering_workspace_size(n, a.size) < 12 * a.size
+    for P in (59, 80):
+        nc, labels = sp_sl_lifetime_csr(indptr, b.astype(np.int32), w, n, P)
+        nc2, lab2 = oracle.sp_sl_lifetime(n, a, b, w, P)
+        assert nc == nc2
+        if nc > 1:
+            assert np.array_equal(labels, lab2)
