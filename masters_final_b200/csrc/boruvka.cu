@@ -966,6 +966,7 @@ struct Engine {
             EACB_CUDA(cudaStreamSynchronize(st));
             if (e) return dev_err_to_status(e);
             if (Ep > Emax) return EACB_ERR_INTERNAL;
+            if (prof().enabled) prof().bytes[PROF_PHASE] += 8.0 * (double)Ep;   // words written
             int64_t nm = 0, nc = 0;
             if ((s = run<SEL_MST>(pk, Ep, V, st, &nm, &nc))) return s;
             mst_base += nm;
@@ -1275,11 +1276,15 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
         // a phase holds a subset of the E entries: the edge array always fits
         auto build = [&](const Phase &ph) -> int {
             if (E == 0) return EACB_OK;
+            ProfScope ps(PROF_PHASE, st);
             k_phase_csr<WT><<<gr, kPhThreads, 0, st>>>(
                 first, deg, dest, weight, V, E, wbits, ph.lo, ph.hi, g.label, pk, g.ea,
                 (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best,
                 g.err);
             EACB_CHECK_LAUNCH();
+            // compulsory reads: row extents and labels (12 B per row), dest and
+            // weight (4 + sizeof(WT) B per entry); the written words follow
+            ps.done(12.0 * V + (4.0 + sizeof(WT)) * (double)E);
             return EACB_OK;
         };
         if ((s = g.run_phased(pk, plan, build, st, &n_mst, &n_comp))) return s;
@@ -1610,10 +1615,16 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
     if ((s = plan_final_phases(wh, g.Emax / 2, indptr, n, st, phases))) return s;
     auto build = [&](const Phase &ph) -> int {
         if (nnz == 0) return EACB_OK;
+        ProfScope ps(PROF_PHASE, st);
         k_phase_upper<<<grid_for((ph.r1 - ph.r0) * 32, kPhThreads), kPhThreads, 0, st>>>(
             indptr, indices, diassoc, n, nnz, ph.lo, ph.hi, ph.r0, ph.r1, g.label, pk, g.ea,
             (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best, g.err);
         EACB_CHECK_LAUNCH();
+        // compulsory reads: row pointers and labels (12 B per row), column and
+        // weight (5 B per entry; a row-range phase is counted in proportion to
+        // its rows); the written words follow
+        const double rows = (double)(ph.r1 - ph.r0);
+        ps.done(12.0 * rows + 5.0 * (double)nnz * (rows / (double)n));
         return EACB_OK;
     };
     if ((s = g.run_phased(pk, phases, build, st, &n_mst, &n_comp))) return s;

@@ -55,6 +55,7 @@ struct CoWS {
     int32_t *order;       // P processing order
     int32_t *rowcnt;      // n kept columns per row
     int32_t *rowflag;     // n: 1 = distinct columns exceed the capacity
+    int32_t *rowperm;     // n: the order the row kernels take rows in
     int *queue;           // 4 row-queue counters
     unsigned long long *disc;   // discarded counts
     int *maxcnt;          // largest kept count
@@ -75,6 +76,7 @@ struct CoWS {
         w.order = c.take<int32_t>(P > 0 ? P : 1);
         w.rowcnt = c.take<int32_t>(n);
         w.rowflag = c.take<int32_t>(n);
+        w.rowperm = c.take<int32_t>(n);
         w.queue = c.take<int>(4);
         w.disc = c.take<unsigned long long>(1);
         w.maxcnt = c.take<int>(1);
@@ -157,8 +159,8 @@ __device__ __forceinline__ void stream_chunk(const int32_t *members, int64_t *ts
 
 // ---------------------------------------------------------------- pass 1 --
 __global__ void __launch_bounds__(kRowThreads)
-k_rows_count(TailCtx tc, const int32_t *order, const int64_t *cap_indptr, int32_t *rowcnt,
-             int32_t *rowflag, int *queue, int *err)
+k_rows_count(TailCtx tc, const int32_t *order, const int32_t *rowperm, const int64_t *cap_indptr,
+             int32_t *rowcnt, int32_t *rowflag, int *queue, int *err)
 {
     extern __shared__ uint32_t bm[];
     __shared__ int64_t ts[kMaxP], te[kMaxP];
@@ -166,8 +168,9 @@ k_rows_count(TailCtx tc, const int32_t *order, const int64_t *cap_indptr, int32_
     const int32_t n = tc.n, P = tc.P;
     constexpr int32_t kCols = kBitmapBytes * 8;
     while (true) {
-        const int i = next_row(queue, &s_row);
-        if (i >= n) break;
+        const int qi = next_row(queue, &s_row);
+        if (qi >= n) break;
+        const int i = rowperm[qi];
         const int64_t cap = cap_indptr[i + 1] - cap_indptr[i];
         for (int p = threadIdx.x; p < P; p += blockDim.x) {
             int64_t s, e;
@@ -248,8 +251,8 @@ __device__ __forceinline__ int64_t emit_chunk(const uint8_t *ctr, int width, int
 }
 
 __global__ void __launch_bounds__(kRowThreads)
-k_rows_fill(TailCtx tc, const int32_t *rowflag, const int64_t *indptr, int32_t *indices,
-            uint8_t *data, int *queue, int *gmax, int *err)
+k_rows_fill(TailCtx tc, const int32_t *rowperm, const int32_t *rowflag, const int64_t *indptr,
+            int32_t *indices, uint8_t *data, int *queue, int *gmax, int *err)
 {
     extern __shared__ uint32_t ctr32[];
     __shared__ int64_t ts[kMaxP], te[kMaxP];
@@ -258,8 +261,9 @@ k_rows_fill(TailCtx tc, const int32_t *rowflag, const int64_t *indptr, int32_t *
     constexpr int32_t kCols = kCountBytes;
     int maxc = 0;
     while (true) {
-        const int i = next_row(queue, &s_row);
-        if (i >= n) break;
+        const int qi = next_row(queue, &s_row);
+        if (qi >= n) break;
+        const int i = rowperm[qi];
         if (rowflag[i]) continue;            // uniform across the block
         for (int p = threadIdx.x; p < P; p += blockDim.x) {
             int64_t s, e;
@@ -303,9 +307,9 @@ k_rows_fill(TailCtx tc, const int32_t *rowflag, const int64_t *indptr, int32_t *
 // rank < r* and the first `quota` rank-r* columns in column order.  A row
 // whose tail span fits one chunk keeps its pass-0 chunk for pass 1.
 __global__ void __launch_bounds__(kRowThreads)
-k_rows_capped(TailCtx tc, const int32_t *order, const int32_t *rowflag, const int64_t *cap_indptr,
-              const int64_t *indptr, int32_t *indices, uint8_t *data, int *queue, int *gmax,
-              unsigned long long *disc, int *err)
+k_rows_capped(TailCtx tc, const int32_t *order, const int32_t *rowperm, const int32_t *rowflag,
+              const int64_t *cap_indptr, const int64_t *indptr, int32_t *indices, uint8_t *data,
+              int *queue, int *gmax, unsigned long long *disc, int *err)
 {
     extern __shared__ uint32_t sm[];
     uint32_t *ctr32 = sm;                      // kCapCols byte counters
@@ -317,8 +321,9 @@ k_rows_capped(TailCtx tc, const int32_t *order, const int32_t *rowflag, const in
     const int32_t n = tc.n, P = tc.P;
     int maxc = 0;
     while (true) {
-        const int i = next_row(queue, &s_row);
-        if (i >= n) break;
+        const int qi = next_row(queue, &s_row);
+        if (qi >= n) break;
+        const int i = rowperm[qi];
         if (!rowflag[i]) continue;
         const int64_t cap = cap_indptr[i + 1] - cap_indptr[i];
         const bool one_chunk = (int64_t)n - ((int64_t)i + 1) <= kCapCols;
@@ -437,6 +442,26 @@ __global__ void k_diassoc(uint8_t *data, int64_t nnz, const int *gmax)
         data[e] = (uint8_t)(top - data[e]);
 }
 
+// Row order of the row kernels: the points cluster by cluster of the
+// partition with the most clusters (its member lists), then the points it
+// leaves unlabelled.  Rows in flight then share member lists -- in that
+// partition by construction, in the others mostly, since they are close
+// points -- and read them from L2 instead of HBM.
+__global__ void k_rowperm(const int32_t *labels, int32_t n, int32_t P, int32_t K, int64_t ntiles,
+                          const int32_t *members, const int64_t *S, const int32_t *ncl,
+                          int32_t *rowperm, int *counter)
+{
+    int pr = 0;
+    for (int p = 1; p < P; ++p)
+        if (ncl[p] > ncl[pr]) pr = p;
+    const int64_t s0 = S[(int64_t)pr * K * ntiles], s1 = S[((int64_t)pr + 1) * K * ntiles];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < s1 - s0; q += stride)
+        rowperm[q] = members[s0 + q];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        if (labels[(int64_t)pr * n + i] < 0) rowperm[(s1 - s0) + atomicAdd(counter, 1)] = (int32_t)i;
+}
+
 static int check_args(const int32_t *labels, int32_t n, int32_t P, int32_t K)
 {
     if (!labels || n <= 0 || P <= 0 || P > kMaxP || K <= 0) return EACB_ERR_BAD_ARGUMENT;
@@ -501,6 +526,9 @@ extern "C" int eacb_coassoc_prepare(const int32_t *labels, int32_t n, int32_t P,
     EACB_CHECK_LAUNCH();
     k_order<<<1, 32, 0, st>>>(w.ncl, P, w.order);
     EACB_CHECK_LAUNCH();
+    k_rowperm<<<grid_for(n, 256), 256, 0, st>>>(labels, n, P, K, nt, w.members, w.S, w.ncl,
+                                                 w.rowperm, &w.queue[3]);
+    EACB_CHECK_LAUNCH();
     int mc = 0;
     EACB_CUDA(cudaMemcpyAsync(&mc, w.maxcnt, sizeof(int), cudaMemcpyDeviceToHost, st));
     if ((s = read_err(w.err, st))) return s;
@@ -523,8 +551,8 @@ extern "C" int eacb_coassoc_count(const int32_t *labels, int32_t n, int32_t P, i
     TailCtx tc{labels, w.members, w.mypos, w.S, n, P, K, w.ntiles};
     EACB_CUDA(allow_max_dyn_smem(k_rows_count));
     ProfScope ps(PROF_COASSOC, st);
-    k_rows_count<<<row_grid(), kRowThreads, kBitmapBytes, st>>>(tc, w.order, cap_indptr, w.rowcnt,
-                                                                 w.rowflag, &w.queue[0], w.err);
+    k_rows_count<<<row_grid(), kRowThreads, kBitmapBytes, st>>>(
+        tc, w.order, w.rowperm, cap_indptr, w.rowcnt, w.rowflag, &w.queue[0], w.err);
     EACB_CHECK_LAUNCH();
     ps.done(0.0);
     if ((s = scan_launch<int32_t, int64_t>(w.rowcnt, indptr, n, 0, &indptr[n], w.scan, st))) return s;
@@ -622,13 +650,13 @@ extern "C" int eacb_coassoc_fill(const int32_t *labels, int32_t n, int32_t P, in
     EACB_CUDA(allow_max_dyn_smem(k_rows_fill));
     EACB_CUDA(allow_max_dyn_smem(k_rows_capped));
     ProfScope ps(PROF_COASSOC, st);
-    k_rows_fill<<<row_grid(), kRowThreads, kCountBytes, st>>>(tc, w.rowflag, indptr, indices, data,
-                                                               &w.queue[1], w.maxcnt, w.err);
+    k_rows_fill<<<row_grid(), kRowThreads, kCountBytes, st>>>(
+        tc, w.rowperm, w.rowflag, indptr, indices, data, &w.queue[1], w.maxcnt, w.err);
     EACB_CHECK_LAUNCH();
     ps.done(0.0);
     k_rows_capped<<<row_grid(), kRowThreads, kCapSmem, st>>>(
-        tc, w.order, w.rowflag, cap_indptr, indptr, indices, data, &w.queue[2], w.maxcnt, w.disc,
-        w.err);
+        tc, w.order, w.rowperm, w.rowflag, cap_indptr, indptr, indices, data, &w.queue[2],
+        w.maxcnt, w.disc, w.err);
     EACB_CHECK_LAUNCH();
     int64_t nnz = 0;
     EACB_CUDA(cudaMemcpyAsync(&nnz, &indptr[n], sizeof(int64_t), cudaMemcpyDeviceToHost, st));

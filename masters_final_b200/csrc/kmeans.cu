@@ -298,35 +298,212 @@ __global__ void k_centroids(const float *__restrict__ X, int32_t n, int32_t D,
 }
 
 // Empty clusters take the points arg_k_select returns for their number
-// (KMeans.py:727-750): the reference's quickselect, one thread per partition.
-__global__ void k_fill_empty(const float *X, int32_t n, int32_t D, const float *dists,
-                             const int64_t *S, int32_t K, int64_t ntiles, const int32_t *kk,
-                             int32_t kmax, const int32_t *active, const int32_t *nempty,
-                             int32_t *args_all, float *C, int *err)
+// (KMeans.py:727-750, MyML/MyML/utils/sorting.py:9-47): the reference's
+// quickselect on (distance, index) pairs, one block per partition, with the
+// distances permuted in place (key[r] is the reference's a[args[r]]; the
+// distances are not needed again before the next label pass).
+//
+// One partition step of the reference on [lo, hi] with pivot mid moves the
+// element at r to the back (swapping in the element at w) when it is >= mid,
+// and otherwise advances r.  Its result has a closed form that a block can
+// compute in parallel.  Read the range from the front (F[t] = position
+// lo + t) and from the back (B[u] = position hi - u); "big" means >= mid.
+// The step examines F up to its m-th big a_m, then B up to its m-th small
+// b_m, then F again, and so on, until hi - lo + 1 elements are examined; the
+// last one examined stays at r.  Every other examined element lands at:
+//   a front small F[t]       -> position of F[t] (it stays),
+//   the m-th front big       -> position of B[b_{m-1} + 1]   (b_0 = -1),
+//   the m-th back small      -> position of F[a_m],
+//   a back big B[u]          -> position of B[u + 1],
+// and r = lo + (number of smalls that landed).  Ranges up to kFillSeqMax
+// elements finish with the reference's loop on one thread.
+constexpr int kFillThreads = 1024;
+constexpr int kFillItems = 8;
+constexpr int64_t kFillSeqMax = 16384;
+constexpr int64_t kFillInf = (int64_t)1 << 62;
+
+// Walks [lo, hi] in ascending order, calling f(p, big, bigs_before) for every
+// position (bigs_before = # bigs in [lo, p)); returns the number of bigs.
+// Called by the whole block.
+template <typename F>
+__device__ int64_t fill_scan_bigs(const float *key, int64_t lo, int64_t hi, float mid, F f)
 {
+    int64_t base = 0;
+    for (int64_t t0 = lo; t0 <= hi; t0 += (int64_t)kFillThreads * kFillItems) {
+        const int64_t p0 = t0 + (int64_t)threadIdx.x * kFillItems;
+        unsigned mask = 0;
+        int c = 0;
+#pragma unroll
+        for (int q = 0; q < kFillItems; ++q) {
+            const int64_t p = p0 + q;
+            if (p <= hi && key[p] >= mid) {
+                mask |= 1u << q;
+                ++c;
+            }
+        }
+        int64_t tot;
+        int64_t before = base + block_excl_sum<kFillThreads>(c, tot);
+#pragma unroll
+        for (int q = 0; q < kFillItems; ++q) {
+            const int64_t p = p0 + q;
+            if (p <= hi) {
+                const bool big = (mask >> q) & 1u;
+                f(p, big, before);
+                before += big;
+            }
+        }
+        base += tot;
+    }
+    return base;
+}
+
+// number of entries <= v in the ascending array a[0, len)
+__device__ __forceinline__ int64_t count_le(const int32_t *a, int64_t len, int64_t v)
+{
+    int64_t lo = 0, hi = len;
+    while (lo < hi) {
+        const int64_t m = (lo + hi) >> 1;
+        if (a[m] <= v) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kFillThreads)
+k_fill_empty(const float *X, int32_t n, int32_t D, float *dists, const int64_t *S, int32_t K,
+             int64_t ntiles, const int32_t *kk, int32_t kmax, const int32_t *active,
+             const int32_t *nempty, int32_t *args_all, int32_t *sel_all, float *okey_all,
+             int32_t *oarg_all, float *C, int *err)
+{
+    __shared__ int64_t s_v[5];
     const int p = blockIdx.x;
-    if (threadIdx.x != 0 || !active[p] || nempty[p] == 0) return;
+    if (!active[p] || nempty[p] == 0) return;          // uniform across the block
     const int k = nempty[p];
-    const float *a = dists + (int64_t)p * n;
+    float *key = dists + (int64_t)p * n;
     int32_t *args = args_all + (int64_t)p * n;
-    for (int64_t i = 0; i < n; ++i) args[i] = (int32_t)i;
-    int64_t lo = 0, hi = n - 1, guard = 0;
+    int32_t *sel = sel_all + (int64_t)p * n;           // front-big and back-small indices
+    float *okey = okey_all + (int64_t)p * n;
+    int32_t *oarg = oarg_all + (int64_t)p * n;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) args[i] = (int32_t)i;
+    __syncthreads();
+    int64_t lo = 0, hi = n - 1;
+    int rounds = 0;
+    while (hi - lo + 1 > kFillSeqMax) {
+        if (++rounds > 4096) {                         // cannot happen: every step shrinks the range
+            if (threadIdx.x == 0) set_err(err, DEV_CHASE_LIMIT);
+            return;
+        }
+        const int64_t L = hi - lo + 1;
+        const float mid = key[(lo + hi) / 2];
+        // count the bigs, then list front bigs (sel[0, NB)) and back smalls
+        // (sel[NB, L)) by rank
+        int64_t nbig;
+        {
+            int64_t c = 0;
+            for (int64_t q = lo + threadIdx.x; q <= hi; q += blockDim.x) c += key[q] >= mid;
+            nbig = 0;
+            block_excl_sum<kFillThreads>(c, nbig);
+        }
+        const int64_t NB = nbig, NS = L - NB;
+        fill_scan_bigs(key, lo, hi, mid, [&](int64_t q, bool big, int64_t before) {
+            const int64_t t = q - lo;
+            if (big) sel[before] = (int32_t)t;
+            else sel[NB + NS - 1 - (t - before)] = (int32_t)(hi - q);   // rank from the back
+        });
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int32_t *A = sel, *Bs = sel + NB;
+            auto a_of = [&](int64_t m) -> int64_t { return m <= NB ? A[m - 1] : kFillInf; };
+            auto b_of = [&](int64_t m) -> int64_t {
+                return m == 0 ? -1 : (m <= NS ? Bs[m - 1] : kFillInf);
+            };
+            // the segment m1 in which the examination ends: first m with
+            // (a_m + 1) + (b_m + 1) >= L
+            int64_t ml = 1, mh = (NB < NS ? NB : NS) + 1;
+            while (ml < mh) {
+                const int64_t m = (ml + mh) >> 1;
+                const int64_t am = a_of(m), bm = b_of(m);
+                const bool reach = am >= kFillInf || bm >= kFillInf || am + bm + 2 >= L;
+                if (reach) mh = m; else ml = m + 1;
+            }
+            const int64_t m1 = ml, am1 = a_of(m1), bprev = b_of(m1 - 1);
+            int64_t x, y, last_front;
+            if (am1 >= kFillInf || am1 + 1 + bprev + 1 >= L) {   // ends in the front run
+                y = bprev;
+                x = L - 2 - y;
+                last_front = 1;
+            } else {                                              // ends in the back run
+                x = am1;
+                y = L - 2 - x;
+                last_front = 0;
+            }
+            const int64_t front_smalls = (x + 1) - count_le(A, NB, x);
+            const int64_t back_smalls = count_le(Bs, NS, y);
+            const int64_t lp = last_front ? lo + x : hi - y;
+            const int64_t settled_smalls = front_smalls + back_smalls - (key[lp] < mid ? 1 : 0);
+            s_v[0] = x;
+            s_v[1] = y;
+            s_v[2] = last_front;
+            s_v[3] = settled_smalls;
+        }
+        __syncthreads();
+        const int64_t x = s_v[0], y = s_v[1], last_front = s_v[2], Sm = s_v[3];
+        fill_scan_bigs(key, lo, hi, mid, [&](int64_t q, bool big, int64_t before) {
+            const int64_t t = q - lo, u = hi - q;
+            const bool front = t <= x;
+            int64_t dst;
+            if ((front && last_front && t == x) || (!front && !last_front && u == y)) {
+                dst = Sm;
+            } else if (front) {
+                if (!big) {
+                    dst = t;
+                } else {                       // the m-th front big, m = before + 1
+                    const int64_t bm = before == 0 ? -1 : sel[NB + before - 1];
+                    dst = (L - 1) - (bm + 1);
+                }
+            } else {
+                if (!big) {                    // back small of rank (from the back)
+                    const int64_t rank = NS - 1 - (t - before);
+                    dst = sel[rank];
+                } else {
+                    dst = (L - 1) - (u + 1);
+                }
+            }
+            okey[lo + dst] = key[q];
+            oarg[lo + dst] = args[q];
+        });
+        __syncthreads();
+        for (int64_t q = lo + threadIdx.x; q <= hi; q += blockDim.x) {
+            key[q] = okey[q];
+            args[q] = oarg[q];
+        }
+        __syncthreads();
+        int64_t r = lo + Sm;
+        if (key[r] > mid) r--;
+        if (k <= r) hi = r; else lo = r + 1;
+    }
+    if (threadIdx.x != 0) return;
+    int64_t guard = 0;
     const int64_t limit = 64 * (int64_t)n + 4096;
     while (lo < hi) {
         int64_t r = lo, w = hi;
-        const float mid = a[args[(r + w) / 2]];
+        const float mid = key[(r + w) / 2];
+        float kr = key[r];
         while (r < w) {
-            if (a[args[r]] >= mid) {
+            if (kr >= mid) {
+                const float kw = key[w];
                 const int32_t t = args[w];
+                key[w] = kr;
                 args[w] = args[r];
+                key[r] = kw;
                 args[r] = t;
+                kr = kw;
                 w--;
             } else {
-                r++;
+                kr = key[++r];
             }
             ++guard;
         }
-        if (a[args[r]] > mid) r--;
+        if (key[r] > mid) r--;
         if (k <= r) hi = r; else lo = r + 1;
         if (++guard > limit) { set_err(err, DEV_CHASE_LIMIT); return; }
     }
@@ -503,8 +680,11 @@ extern "C" int eacb_kmeans_ensemble(const float *X, int32_t n, int32_t d, int32_
             k_centroids<false><<<cg, 256, 0, st>>>(X, n, d, w.members, w.S, kmax, nt, k, kmax,
                                                    w.active, centroids, w.nempty);
         EACB_CHECK_LAUNCH();
-        k_fill_empty<<<P, 32, 0, st>>>(X, n, d, w.dists, w.S, kmax, nt, k, kmax, w.active, w.nempty,
-                                       w.args, centroids, w.err);
+        // amb, mypos and members are free here (the centroids are done) and
+        // serve as the quickselect's scratch
+        k_fill_empty<<<P, kFillThreads, 0, st>>>(X, n, d, w.dists, w.S, kmax, nt, k, kmax,
+                                                 w.active, w.nempty, w.args, w.amb,
+                                                 (float *)w.mypos, w.members, centroids, w.err);
         EACB_CHECK_LAUNCH();
     }
     if (dists_out)

@@ -78,6 +78,28 @@ def test_fit_f64_centroids_and_empty_clusters(T):
             assert int(it[p].item()) == ri
 
 
+def test_fit_empty_clusters_large_n(T):
+    """Empty clusters with n above the one-thread limit of the quickselect:
+    the block-parallel partition steps must reproduce the reference's
+    selection order exactly (ten duplicated initial points, so ten clusters
+    empty out in the first pass)."""
+    from masters_final_b200.cluster.KMeans import kmeans_ensemble
+    rng = np.random.default_rng(12)
+    n = 120_000
+    x = rng.standard_normal((n, 4)).astype(np.float32)
+    x[1:20:2] = x[0:20:2]
+    x[5000:5010] = x[7]                  # ties among the distances as well
+    inits = [list(range(20)) + list(rng.choice(np.arange(20, n), 44, replace=False)),
+             list(range(0, 20, 2)) + list(range(1, 20, 2)) + list(range(20, 40))]
+    ks = [64, 40]
+    lab, cent, dist, it, inertia = kmeans_ensemble(x, ks, inits, max_iter=4)
+    for p in range(2):
+        rl, rc, ri = oracle.kmeans_fit(x, ks[p], inits[p], max_iter=4)
+        assert np.array_equal(lab[p].cpu().numpy(), rl)
+        assert np.array_equal(cent[p, :ks[p]].cpu().numpy(), rc)
+        assert int(it[p].item()) == ri
+
+
 @pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("name", ["eac_small", "eac_discard", "eac_10k"])
 def test_ensemble_golden(T, mode, name):
