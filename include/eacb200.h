@@ -180,6 +180,28 @@ int eacb_kmeans_label(const float *X, int32_t n, int32_t d, const float *C, int3
                       int32_t label_mode, int32_t *labels, float *dists,
                       void *ws, size_t ws_bytes, uintptr_t stream);
 
+/* The label step with its arithmetic path fixed by name: float32 screen on
+ * CUDA cores, or tcgen05 BF16 tensor cores; both with the exact re-check,
+ * so both return the reference's labels and distances.  Workspace as for
+ * eacb_kmeans_label. */
+int eacb_kmeans_label_fp32(const float *X, int32_t n, int32_t d, const float *C, int32_t k,
+                           int32_t *labels, float *dists, void *ws, size_t ws_bytes,
+                           uintptr_t stream);
+int eacb_kmeans_label_bf16tc(const float *X, int32_t n, int32_t d, const float *C, int32_t k,
+                             int32_t *labels, float *dists, void *ws, size_t ws_bytes,
+                             uintptr_t stream);
+
+/* One centroid update, MyML/MyML/cluster/KMeans.py:709-754
+ * (numba_recompute_centroids): C (k x d float32) receives, per cluster, the
+ * float32 sum of its points in point order (centroid_mode 1: float64 sums)
+ * divided as f32(f64(sum) / count); empty clusters take, in cluster order,
+ * the points arg_k_select (MyML/MyML/utils/sorting.py:9-47) returns for
+ * their number from `dists` (n float32, left unchanged).  labels in [0, k). */
+size_t eacb_kmeans_centroids_workspace_size(int32_t n, int32_t d, int32_t k);
+int eacb_kmeans_centroids(const float *X, int32_t n, int32_t d, const int32_t *labels,
+                          const float *dists, int32_t k, int32_t centroid_mode, float *C,
+                          void *ws, size_t ws_bytes, uintptr_t stream);
+
 /* ------------------------------------------------------------------------
  * Sparse co-association matrix, condensed (row i holds columns j > i).
  * Replaces MyML/MyML/EAC/sparse.py:154-226 (EAC_CSR.update_ensemble with
@@ -215,6 +237,20 @@ int eacb_coassoc_fill(const int32_t *labels, int32_t n, int32_t P, int32_t K,
                       int32_t *indices, uint8_t *data, int32_t make_diassoc,
                       int64_t *host_discarded, int32_t *host_max_count,
                       void *ws, size_t ws_bytes, uintptr_t stream);
+
+/* The whole build in one call, as EAC.buildMatrix runs it
+ * (MyML/MyML/EAC/eac.py:115-140): member lists, then the capacity layout
+ * (cap_mode 0 = indptr_linear with its default line, 1 = indptr_constant)
+ * for max_assocs (0: factor x the largest cluster), then counts and rows.
+ * indices/data have room for `capacity` entries (the reference preallocates
+ * the layout's total; the kept count never exceeds it).  *host_nnz,
+ * *host_discarded, *host_max_count and *host_max_assocs are set. */
+size_t eacb_coassoc_build_workspace_size(int32_t n, int32_t P, int32_t K);
+int eacb_coassoc_build(const int32_t *labels, int32_t n, int32_t P, int32_t K, int32_t cap_mode,
+                       int64_t max_assocs, int32_t factor, int64_t *indptr, int32_t *indices,
+                       uint8_t *data, int64_t capacity, int32_t make_diassoc, int64_t *host_nnz,
+                       int64_t *host_discarded, int32_t *host_max_count,
+                       int64_t *host_max_assocs, void *ws, size_t ws_bytes, uintptr_t stream);
 
 /* Per-row capacity layouts of the co-association rows (exclusive scan of
  * the capacities, n+1 int64).  Replaces MyML/MyML/EAC/sparse.py:371-413
@@ -254,6 +290,25 @@ int eacb_final_clustering(const int64_t *indptr, const int32_t *indices,
                           int32_t *labels, int64_t *host_n_fclusts,
                           int32_t *host_labels_valid,
                           void *ws, size_t ws_bytes, uintptr_t stream);
+
+/* The final clustering's two steps as separate calls.
+ * eacb_lifetime_cut: lifetime_n_clusters (MyML/MyML/EAC/eac.py:366-391) and
+ * the cut decision of sp_sl_lifetime (:220-265) on the uint8 weights of a
+ * minimum spanning forest of n points (n_mst < n weights, any order);
+ * *host_n_clusters receives the number of clusters and *host_threshold the
+ * largest forest weight kept (-1 keeps none).  EACB_ERR_VALUE where the
+ * reference raises ValueError.
+ * eacb_relabel_canonical: numbers the groups of a labelling (n ids in
+ * [0, n)) by their smallest member, the numbering of scipy's
+ * connected_components that the final labels use; labels_out may equal
+ * labels_in; *host_n_groups receives the number of groups. */
+size_t eacb_lifetime_cut_workspace_size(void);
+int eacb_lifetime_cut(const uint8_t *mst_weights, int64_t n_mst, int32_t n, int32_t max_dist,
+                      int32_t n_clusters, int64_t *host_n_clusters, int32_t *host_threshold,
+                      void *ws, size_t ws_bytes, uintptr_t stream);
+size_t eacb_relabel_canonical_workspace_size(int32_t n);
+int eacb_relabel_canonical(const int32_t *labels_in, int32_t n, int32_t *labels_out,
+                           int64_t *host_n_groups, void *ws, size_t ws_bytes, uintptr_t stream);
 
 /* ------------------------------------------------------------------------
  * Batched EAC: many independent instances, each the whole path above

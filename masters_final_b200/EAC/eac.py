@@ -75,6 +75,42 @@ def lifetime_n_clusters(weights):
     return cont, th
 
 
+def lifetime_cut_gpu(mst_weights, n_samples, max_dist, n_clusters=0, stream=None):
+    """The lifetime rule and cut decision of sp_sl_lifetime on the device
+    (MyML/MyML/EAC/eac.py:220-265, 366-391): (number of clusters, largest
+    forest weight kept) for the uint8 weights of a minimum spanning forest of
+    n_samples points.  Raises ValueError where the reference does."""
+    t = _lib.torch()
+    W = _lib.to_device(mst_weights, t.uint8)
+    L = _lib.load()
+    ws = _lib.workspace(L.eacb_lifetime_cut_workspace_size())
+    nc, th = ctypes.c_int64(0), ctypes.c_int32(0)
+    st = L.eacb_lifetime_cut(_lib.ptr(W), int(W.numel()), int(n_samples), int(max_dist),
+                             int(n_clusters), ctypes.byref(nc), ctypes.byref(th), _lib.ptr(ws),
+                             ws.numel(), _lib.stream_handle(stream))
+    if st == _lib.ERR_VALUE:
+        raise ValueError("lifetime rule undefined: fewer than two MST edges or no two MST "
+                         "edges of equal weight (the reference raises here too)")
+    _lib.check(st, "lifetime cut")
+    return int(nc.value), int(th.value)
+
+
+def relabel_canonical(labels, stream=None):
+    """Numbers groups by their smallest member (scipy connected_components'
+    numbering); returns (device int32 labels, number of groups)."""
+    t = _lib.torch()
+    Ld = _lib.to_device(labels, t.int32)
+    n = int(Ld.numel())
+    out = t.empty_like(Ld)
+    L = _lib.load()
+    ws = _lib.workspace(L.eacb_relabel_canonical_workspace_size(n))
+    ng = ctypes.c_int64(0)
+    _lib.check(L.eacb_relabel_canonical(_lib.ptr(Ld), n, _lib.ptr(out), ctypes.byref(ng),
+                                        _lib.ptr(ws), ws.numel(), _lib.stream_handle(stream)),
+               "relabel")
+    return out, int(ng.value)
+
+
 class EAC:
     """Evidence accumulation clustering (MyML/MyML/EAC/eac.py:40-179).
 

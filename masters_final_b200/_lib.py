@@ -77,6 +77,17 @@ def load():
         "eacb_make_diassoc": (ctypes.c_int, [p, i64, i32, p]),
         "eacb_coassoc_fill": (ctypes.c_int, [p, i32, i32, i32, p, p, p, p, i32, P64, P32, p, sz,
                                              p]),
+        "eacb_kmeans_label_fp32": (ctypes.c_int, [p, i32, i32, p, i32, p, p, p, sz, p]),
+        "eacb_kmeans_label_bf16tc": (ctypes.c_int, [p, i32, i32, p, i32, p, p, p, sz, p]),
+        "eacb_kmeans_centroids_workspace_size": (sz, [i32, i32, i32]),
+        "eacb_kmeans_centroids": (ctypes.c_int, [p, i32, i32, p, p, i32, i32, p, p, sz, p]),
+        "eacb_coassoc_build_workspace_size": (sz, [i32, i32, i32]),
+        "eacb_coassoc_build": (ctypes.c_int, [p, i32, i32, i32, i32, i64, i32, p, p, p, i64, i32,
+                                              P64, P64, P32, P64, p, sz, p]),
+        "eacb_lifetime_cut_workspace_size": (sz, []),
+        "eacb_lifetime_cut": (ctypes.c_int, [p, i64, i32, i32, i32, P64, P32, p, sz, p]),
+        "eacb_relabel_canonical_workspace_size": (sz, [i32]),
+        "eacb_relabel_canonical": (ctypes.c_int, [p, i32, p, P64, p, sz, p]),
         "eacb_batched_workspace_size": (sz, [p, i32, i32]),
         "eacb_batched_eac": (ctypes.c_int, [p, i32, p, i32, p, sz, p]),
         "eacb_final_clustering_workspace_size": (sz, [i32, i64]),

@@ -75,6 +75,24 @@ def kmeans_label(X, centroids, label_mode="cuda", stream=None):
     return labels, dists
 
 
+def kmeans_centroids(X, labels, dists, k, centroid_mode="numba", stream=None):
+    """One centroid update (MyML/MyML/cluster/KMeans.py:709-754): a (k, d)
+    float32 device tensor; empty clusters take the points the reference's
+    quickselect picks from ``dists``."""
+    t = _lib.torch()
+    Xd = _lib.to_device(X, t.float32)
+    Ld = _lib.to_device(labels, t.int32)
+    Dd = _lib.to_device(dists, t.float32)
+    n, d = int(Xd.shape[0]), int(Xd.shape[1])
+    C = t.empty((int(k), d), dtype=t.float32, device=Xd.device)
+    L = _lib.load()
+    ws = _lib.workspace(L.eacb_kmeans_centroids_workspace_size(n, d, int(k)))
+    _lib.check(L.eacb_kmeans_centroids(_lib.ptr(Xd), n, d, _lib.ptr(Ld), _lib.ptr(Dd), int(k),
+                                       _CENTROID[centroid_mode], _lib.ptr(C), _lib.ptr(ws),
+                                       ws.numel(), _lib.stream_handle(stream)), "kmeans centroids")
+    return C
+
+
 class K_Means:
     """MyML/MyML/cluster/KMeans.py:26 (same arguments and attributes)."""
 

@@ -428,45 +428,60 @@ k_whist_csr(const WT *weight, int64_t E, int wbits, unsigned long long *hist)
     hist_flush(h, hist);
 }
 
-// uint8 weights, 16 per thread per step (128-bit loads)
-__global__ void __launch_bounds__(kHistThreads)
+// uint8 weights, 16 per thread per step (128-bit loads).  Every lane owns a
+// private column of 256 counters (bank = lane, so no conflicts and no
+// atomics): counts[warp][bin][lane], 32 KB per warp, two warps per block.
+constexpr int kHist8Threads = 64;
+constexpr size_t kHist8Smem = (size_t)(kHist8Threads / 32) * 256 * 32 * sizeof(uint32_t);
+__global__ void __launch_bounds__(kHist8Threads)
 k_whist_u8(const uint8_t *w, int64_t n, unsigned long long *hist)
 {
-    __shared__ unsigned h[kHistThreads / 32][256];
-    for (int i = threadIdx.x; i < (kHistThreads / 32) * 256; i += blockDim.x) (&h[0][0])[i] = 0;
+    extern __shared__ uint32_t hs[];
+    for (int i = threadIdx.x; i < (kHist8Threads / 32) * 256 * 32; i += blockDim.x) hs[i] = 0;
     __syncthreads();
-    unsigned *mine = h[threadIdx.x >> 5];
+    uint32_t *mine = hs + (threadIdx.x >> 5) * 256 * 32 + (threadIdx.x & 31);
     int64_t head = (int64_t)((16 - ((uintptr_t)w & 15)) & 15);
     if (head > n) head = n;
     const int64_t nv = (n - head) >> 4;               // whole 16-byte vectors
     const uint4 *v = reinterpret_cast<const uint4 *>(w + head);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t q0 = (int64_t)blockIdx.x * blockDim.x; q0 < nv; q0 += stride) {
-        const int64_t q = q0 + threadIdx.x;
-        const bool ok = q < nv;
-        uint4 x = ok ? __ldcs(v + q) : make_uint4(0, 0, 0, 0);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nv; q += stride) {
+        const uint4 x = __ldcs(v + q);
         const uint32_t wd[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-        for (int k = 0; k < 16; ++k) hist_add(mine, (wd[k >> 2] >> (8 * (k & 3))) & 255u, ok);
+        for (int k = 0; k < 16; ++k) mine[((wd[k >> 2] >> (8 * (k & 3))) & 255u) * 32] += 1;
     }
-    // the unaligned head and the ragged tail, by the first block
+    // the unaligned head and the ragged tail (< 32 bytes), by the first block
     if (blockIdx.x == 0) {
         const int64_t tail0 = head + (nv << 4);
-        const int64_t rest = head + (n - tail0);       // < 32 elements
-        const bool ok = (int64_t)threadIdx.x < rest;
-        int64_t e = threadIdx.x < head ? (int64_t)threadIdx.x : tail0 + (threadIdx.x - head);
-        if (threadIdx.x < 32) hist_add(mine, ok ? w[e] : 0u, ok);
+        const int64_t rest = head + (n - tail0);
+        const int64_t t = threadIdx.x;
+        if (t < rest) mine[(uint32_t)w[t < head ? t : tail0 + (t - head)] * 32] += 1;
     }
-    hist_flush(h, hist);
+    __syncthreads();
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) {
+        unsigned long long tot = 0;
+        for (int wp = 0; wp < kHist8Threads / 32; ++wp)
+            for (int l = 0; l < 32; ++l) tot += hs[(wp * 256 + b) * 32 + l];
+        if (tot) atomicAdd(&hist[b], tot);
+    }
+}
+
+static int launch_whist_u8(const uint8_t *w, int64_t n, unsigned long long *hist, cudaStream_t st)
+{
+    EACB_CUDA(allow_max_dyn_smem(k_whist_u8));
+    k_whist_u8<<<grid_for((n + 15) / 16, kHist8Threads, 148 * 3), kHist8Threads, kHist8Smem,
+                 st>>>(w, n, hist);
+    EACB_CHECK_LAUNCH();
+    return EACB_OK;
 }
 
 // Phase builds: the edges of a weight-bucket range (lo, hi] whose endpoints
 // are in different components, appended to eout, with the first round's
-// minimum-edge selection.  A warp takes a row; the 8 rows of a block reserve
-// their output slots with one atomicAdd per block step (a count pass, then a
-// write pass over the same, now cached, entries), which keeps the shared
-// cursor off the critical path.  Edge order is not deterministic, results
-// are: selection uses a strict total order.
+// minimum-edge selection.  The rows of a block step reserve their output
+// slots with one atomicAdd, which keeps the shared cursor off the critical
+// path.  Edge order is not deterministic, results are: selection uses a
+// strict total order.
 constexpr int kPhThreads = 256;
 constexpr int kPhWarps = kPhThreads / 32;
 
@@ -497,6 +512,28 @@ __device__ __forceinline__ bool phase_reserve(int64_t *s_cnt, unsigned long long
     return s_ok != 0;
 }
 
+// Graph rows are short (degrees): a warp takes kPhRows consecutive rows per
+// block step and stages its kept words in shared memory in one pass; the
+// block then reserves once and copies the staged words out coalesced.  A
+// warp whose staging fills up flushes it on its own (one reservation).
+constexpr int kPhRows = 16;
+constexpr int kPhStage = 512;            // staged words per warp
+
+__device__ __forceinline__ void phase_flush_warp(const uint64_t *stage, int cnt, uint64_t *eout,
+                                                 unsigned long long *cursor,
+                                                 unsigned long long cap, int *err)
+{
+    const int lane = threadIdx.x & 31;
+    unsigned long long b = 0;
+    if (lane == 0) b = atomicAdd(cursor, (unsigned long long)cnt);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if (b + cnt > cap) {
+        if (lane == 0) set_err(err, DEV_CAPACITY);
+        return;
+    }
+    for (int i = lane; i < cnt; i += 32) eout[b + i] = stage[i];
+}
+
 template <typename WT>
 __global__ void __launch_bounds__(kPhThreads)
 k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const WT *weight,
@@ -504,90 +541,76 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
             uint64_t *eout, unsigned long long *cursor, unsigned long long cap,
             unsigned long long *best, int *err)
 {
-    // rows are short (graph degrees): a warp takes kPhRows consecutive rows
-    // per block step, so one reservation covers 8 * kPhRows rows
-    constexpr int kPhRows = 16;
+    __shared__ uint64_t stage_all[kPhWarps][kPhStage];
     __shared__ int64_t s_cnt[kPhWarps];
     __shared__ unsigned long long s_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    auto test = [&](int64_t u, int64_t f, int64_t d, int32_t lu, int64_t e, uint32_t &w,
-                    int32_t &v) -> bool {
-        if (e >= f + d) return false;
-        v = dest[e];
-        if (v < 0 || v >= V) {
-            set_err(err, DEV_BAD_INPUT);
-            return false;
-        }
-        if (v == (int32_t)u) return false;
-        w = wword(weight[e]);
-        const int b = (int)wbucket(w, wbits);
-        return b > lo && b <= hi && label[v] != lu;
-    };
-    auto row = [&](int64_t u, int64_t &f, int64_t &d, int32_t &lu) {
-        f = 0;
-        d = 0;
-        lu = 0;
-        if (u >= V) return;
-        f = first[u];
-        d = deg[u];
-        if (f < 0 || d < 0 || f + d > E) {
-            if (lane == 0) set_err(err, DEV_BAD_INPUT);
-            d = 0;
-            return;
-        }
-        lu = label[u];
-    };
+    uint64_t *stage = stage_all[warp];
     const int64_t step = (int64_t)kPhWarps * kPhRows;
     for (int64_t r0 = (int64_t)blockIdx.x * step; r0 < V; r0 += (int64_t)gridDim.x * step) {
         const int64_t u0 = r0 + (int64_t)warp * kPhRows;
-        int64_t cnt = 0;
+        int cnt = 0;
         for (int r = 0; r < kPhRows; ++r) {
-            int64_t f, d;
-            int32_t lu;
-            row(u0 + r, f, d, lu);
-            for (int64_t e0 = f; e0 < f + d; e0 += 32) {
-                uint32_t w;
-                int32_t v;
-                cnt += __popc(__ballot_sync(0xffffffffu, test(u0 + r, f, d, lu, e0 + lane, w, v)));
+            const int64_t u = u0 + r;
+            if (u >= V) break;                       // warp-uniform
+            int64_t f = first[u], d = deg[u];
+            if (f < 0 || d < 0 || f + d > E) {
+                if (lane == 0) set_err(err, DEV_BAD_INPUT);
+                continue;
             }
+            const int32_t lu = label[u];
+            uint64_t m = kNone;
+            for (int64_t e0 = f; e0 < f + d; e0 += 32) {
+                const int64_t e = e0 + lane;
+                bool keep = false;
+                uint64_t k = 0;
+                if (e < f + d) {
+                    const int32_t v = dest[e];
+                    if (v < 0 || v >= V) {
+                        set_err(err, DEV_BAD_INPUT);
+                    } else if (v != (int32_t)u) {
+                        const uint32_t w = wword(weight[e]);
+                        const int bk = (int)wbucket(w, wbits);
+                        if (bk > lo && bk <= hi && label[v] != lu) {
+                            keep = true;
+                            k = pk.make(w, (uint32_t)u, (uint32_t)v);
+                            m = (k >> 1) < m ? (k >> 1) : m;
+                        }
+                    }
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                const int nb = __popc(bal);
+                if (cnt + nb > kPhStage) {               // staging full: flush it now
+                    __syncwarp();
+                    phase_flush_warp(stage, cnt, eout, cursor, cap, err);
+                    __syncwarp();
+                    cnt = 0;
+                }
+                if (keep) stage[cnt + __popc(bal & lt)] = k;
+                cnt += nb;
+            }
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) {
+                const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
+                m = x < m ? x : m;
+            }
+            if (lane == 0 && m != kNone) min_if_lower(&best[lu], m);
         }
         if (lane == 0) s_cnt[warp] = cnt;
         const bool fits = phase_reserve(s_cnt, &s_base, cursor, 1, cap, err);
-        if (cnt && fits) {
-            unsigned long long at = s_base + (unsigned long long)s_cnt[warp];
-            for (int r = 0; r < kPhRows; ++r) {
-                const int64_t u = u0 + r;
-                int64_t f, d;
-                int32_t lu;
-                row(u, f, d, lu);
-                uint64_t m = kNone;
-                for (int64_t e0 = f; e0 < f + d; e0 += 32) {
-                    uint32_t w = 0;
-                    int32_t v = 0;
-                    const bool keep = test(u, f, d, lu, e0 + lane, w, v);
-                    const unsigned bal = __ballot_sync(0xffffffffu, keep);
-                    if (keep) {
-                        const uint64_t k = pk.make(w, (uint32_t)u, (uint32_t)v);
-                        eout[at + __popc(bal & lt)] = k;
-                        m = (k >> 1) < m ? (k >> 1) : m;
-                    }
-                    at += __popc(bal);
-                }
-#pragma unroll
-                for (int o = 16; o >= 1; o >>= 1) {
-                    const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
-                    m = x < m ? x : m;
-                }
-                if (lane == 0 && m != kNone) min_if_lower(&best[lu], m);
-            }
+        if (fits) {
+            const unsigned long long at = s_base + (unsigned long long)s_cnt[warp];
+            for (int i = lane; i < cnt; i += 32) eout[at + i] = stage[i];
         }
-        __syncthreads();          // s_cnt is rewritten by the next step
+        __syncthreads();          // staging and s_cnt are reused by the next step
     }
 }
 
 // Same for an upper-triangle CSR with uint8 weights: both directions of each
-// kept entry.
+// kept entry.  Co-association rows are long (thousands of entries), so a
+// warp takes one row, counts its kept entries, and after the block's
+// reservation writes them in a second pass over the (now cached) row.
 __global__ void __launch_bounds__(kPhThreads)
 k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, int32_t n,
               int64_t nnz, int lo, int hi, int64_t row0, int64_t row1, const int32_t *label,
@@ -1258,12 +1281,12 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
         // weight phases over the bucket histogram of the entries
         EACB_CUDA(cudaMemsetAsync(g.hist, 0, 256 * sizeof(unsigned long long), st));
         if (E > 0) {
-            if (sizeof(WT) == 1)
-                k_whist_u8<<<grid_for((E + 15) / 16, kHistThreads, 148 * 8), kHistThreads, 0,
-                             st>>>((const uint8_t *)weight, E, g.hist);
-            else
+            if (sizeof(WT) == 1) {
+                if ((s = launch_whist_u8((const uint8_t *)weight, E, g.hist, st))) return s;
+            } else {
                 k_whist_csr<WT><<<grid_for(E, kHistThreads, 148 * 8), kHistThreads, 0, st>>>(
                     weight, E, wbits, g.hist);
+            }
             EACB_CHECK_LAUNCH();
         }
         unsigned long long h[256];
@@ -1604,9 +1627,7 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
     // 1. minimum spanning forest of the dissimilarity graph, by weight phases
     EACB_CUDA(cudaMemsetAsync(g.hist, 0, 256 * sizeof(unsigned long long), st));
     if (nnz > 0) {
-        k_whist_u8<<<grid_for((nnz + 15) / 16, kHistThreads, 148 * 8), kHistThreads, 0, st>>>(
-            diassoc, nnz, g.hist);
-        EACB_CHECK_LAUNCH();
+        if ((s = launch_whist_u8(diassoc, nnz, g.hist, st))) return s;
     }
     int64_t n_mst = 0, n_comp = 0;
     unsigned long long wh[256];
@@ -1672,5 +1693,112 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
     if ((s = g.read_counts(st, h))) return s;
     *host_n_fclusts = h[1];
     *host_labels_valid = 1;
+    return EACB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The final clustering's two steps as separate calls.
+// ---------------------------------------------------------------------------
+__global__ void k_check_labels(const int32_t *labels, int32_t n, int *err)
+{
+    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n;
+         x += (int64_t)gridDim.x * blockDim.x)
+        if (labels[x] < 0 || labels[x] >= n) set_err(err, DEV_BAD_INPUT);
+}
+
+extern "C" size_t eacb_lifetime_cut_workspace_size(void)
+{
+    Carver c(nullptr, 0);
+    c.take<unsigned long long>(256);
+    c.take<CutPlan>(1);
+    return c.off;
+}
+
+// lifetime_n_clusters (MyML/MyML/EAC/eac.py:366-391) and the cut decision of
+// sp_sl_lifetime (:220-265) on the uint8 weights of a minimum spanning forest
+// of n points (any order).  *host_n_clusters receives the number of clusters;
+// *host_threshold the largest forest weight kept (-1: none, 255: all).
+extern "C" int eacb_lifetime_cut(const uint8_t *mst_weights, int64_t n_mst, int32_t n,
+                                 int32_t max_dist, int32_t n_clusters, int64_t *host_n_clusters,
+                                 int32_t *host_threshold, void *ws, size_t ws_bytes,
+                                 uintptr_t stream)
+{
+    if (n <= 0 || n_mst < 0 || n_mst >= n || (n_mst > 0 && !mst_weights) || n_clusters < 0 ||
+        !host_n_clusters || !host_threshold || !ws)
+        return EACB_ERR_BAD_ARGUMENT;
+    cudaStream_t st = as_stream(stream);
+    Carver c(ws, ws_bytes);
+    unsigned long long *hist = c.take<unsigned long long>(256);
+    CutPlan *plan = c.take<CutPlan>(1);
+    if (c.overflow) return EACB_ERR_WORKSPACE;
+    EACB_CUDA(cudaMemsetAsync(hist, 0, 256 * sizeof(unsigned long long), st));
+    if (n_mst > 0) {
+        const int s = launch_whist_u8(mst_weights, n_mst, hist, st);
+        if (s) return s;
+    }
+    k_cut_plan<<<1, 32, 0, st>>>((const int64_t *)hist, n_mst, n, max_dist, n_clusters, plan);
+    EACB_CHECK_LAUNCH();
+    CutPlan hp;
+    EACB_CUDA(cudaMemcpyAsync(&hp, plan, sizeof(CutPlan), cudaMemcpyDeviceToHost, st));
+    EACB_CUDA(cudaStreamSynchronize(st));
+    if (hp.status) return (int)hp.status;
+    *host_n_clusters = hp.n_clusters;
+    *host_threshold = (int32_t)hp.wmax;
+    return EACB_OK;
+}
+
+extern "C" size_t eacb_relabel_canonical_workspace_size(int32_t n)
+{
+    Carver c(nullptr, 0);
+    c.take<int>(1);
+    c.take<int64_t>(1);
+    c.take<int32_t>(n);
+    c.take<int32_t>(n);
+    c.take<int32_t>(n);
+    ScanScratch::carve(c, n);
+    return c.off;
+}
+
+// Numbers the groups of a labelling by their smallest member (the group of
+// point 0 is 0, the next group to appear is 1, ...): the numbering scipy's
+// connected_components gives, which the final labels use.  labels_in holds
+// n group ids in [0, n); labels_out may equal labels_in.
+extern "C" int eacb_relabel_canonical(const int32_t *labels_in, int32_t n, int32_t *labels_out,
+                                      int64_t *host_n_groups, void *ws, size_t ws_bytes,
+                                      uintptr_t stream)
+{
+    if (!labels_in || n <= 0 || !labels_out || !host_n_groups || !ws) return EACB_ERR_BAD_ARGUMENT;
+    cudaStream_t st = as_stream(stream);
+    Carver c(ws, ws_bytes);
+    int *err = c.take<int>(1);
+    int64_t *total = c.take<int64_t>(1);
+    int32_t *cmin = c.take<int32_t>(n);
+    int32_t *flag = c.take<int32_t>(n);
+    int32_t *pos = c.take<int32_t>(n);
+    ScanScratch scan = ScanScratch::carve(c, n, err);
+    if (c.overflow) return EACB_ERR_WORKSPACE;
+    EACB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    EACB_CUDA(cudaMemsetAsync(cmin, 0x7f, sizeof(int32_t) * n, st));
+    const unsigned gn = grid_for(n, 256);
+    k_check_labels<<<gn, 256, 0, st>>>(labels_in, n, err);
+    EACB_CHECK_LAUNCH();
+    int e = 0;
+    EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EACB_CUDA(cudaStreamSynchronize(st));
+    if (e) return dev_err_to_status(e);
+    k_comp_min<<<gn, 256, 0, st>>>(labels_in, n, cmin);
+    EACB_CHECK_LAUNCH();
+    k_first_flag<<<gn, 256, 0, st>>>(labels_in, cmin, n, flag);
+    EACB_CHECK_LAUNCH();
+    int s = scan_launch<int32_t, int32_t>(flag, pos, n, 0, total, scan, st);
+    if (s) return s;
+    k_canon<<<gn, 256, 0, st>>>(labels_in, cmin, pos, n, labels_out);
+    EACB_CHECK_LAUNCH();
+    int64_t ng = 0;
+    EACB_CUDA(cudaMemcpyAsync(&ng, total, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EACB_CUDA(cudaStreamSynchronize(st));
+    if (e) return dev_err_to_status(e);
+    *host_n_groups = ng;
     return EACB_OK;
 }

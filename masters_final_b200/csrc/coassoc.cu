@@ -128,12 +128,18 @@ __device__ __forceinline__ int64_t block_sum(int64_t v)
 // averages a few hundred members); a tail is sorted, so the members below jl
 // are a prefix of the step.
 constexpr int kStreamU = 8;
+// Warps take tails dynamically (*next, zeroed by the caller before the
+// block's barrier), so warps that drew short tails take more of them.
 template <typename Op>
 __device__ __forceinline__ void stream_chunk(const int32_t *members, int64_t *ts, const int64_t *te,
-                                             int32_t P, int32_t jl, Op op)
+                                             int32_t P, int32_t jl, int *next, Op op)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int p = warp; p < P; p += nw) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int p = 0;
+        if (lane == 0) p = atomicAdd(next, 1);
+        p = __shfl_sync(0xffffffffu, p, 0);
+        if (p >= P) break;
         int64_t cur = ts[p];
         const int64_t end = te[p];
         while (cur < end) {
@@ -164,7 +170,7 @@ k_rows_count(TailCtx tc, const int32_t *order, const int32_t *rowperm, const int
 {
     extern __shared__ uint32_t bm[];
     __shared__ int64_t ts[kMaxP], te[kMaxP];
-    __shared__ int s_row;
+    __shared__ int s_row, s_next;
     const int32_t n = tc.n, P = tc.P;
     constexpr int32_t kCols = kBitmapBytes * 8;
     while (true) {
@@ -185,9 +191,10 @@ k_rows_count(TailCtx tc, const int32_t *order, const int32_t *rowperm, const int
             const int32_t jl = (int32_t)((j0 + kCols < n) ? j0 + kCols : n);
             const int nwords = (int)((jl - j0 + 31) >> 5);
             for (int w = threadIdx.x; w < nwords; w += blockDim.x) bm[w] = 0;
+            if (threadIdx.x == 0) s_next = 0;
             __syncthreads();
             const int32_t jb = (int32_t)j0;
-            stream_chunk(tc.members, ts, te, P, jl, [&](int32_t j, int) {
+            stream_chunk(tc.members, ts, te, P, jl, &s_next, [&](int32_t j, int) {
                 const int32_t o = j - jb;
                 atomicOr(&bm[o >> 5], 1u << (o & 31));
             });
@@ -256,7 +263,7 @@ k_rows_fill(TailCtx tc, const int32_t *rowperm, const int32_t *rowflag, const in
 {
     extern __shared__ uint32_t ctr32[];
     __shared__ int64_t ts[kMaxP], te[kMaxP];
-    __shared__ int s_row;
+    __shared__ int s_row, s_next;
     const int32_t n = tc.n, P = tc.P;
     constexpr int32_t kCols = kCountBytes;
     int maxc = 0;
@@ -278,9 +285,10 @@ k_rows_fill(TailCtx tc, const int32_t *rowperm, const int32_t *rowflag, const in
             const int width = (int)(jl - j0);
             const int nwords = (width + 15) >> 4 << 2;
             for (int w = threadIdx.x; w < nwords; w += blockDim.x) ctr32[w] = 0;
+            if (threadIdx.x == 0) s_next = 0;
             __syncthreads();
             const int32_t jb = (int32_t)j0;
-            stream_chunk(tc.members, ts, te, P, jl, [&](int32_t j, int) {
+            stream_chunk(tc.members, ts, te, P, jl, &s_next, [&](int32_t j, int) {
                 const int32_t o = j - jb;
                 atomicAdd(&ctr32[o >> 2], 1u << (8 * (o & 3)));
             });
@@ -317,7 +325,7 @@ k_rows_capped(TailCtx tc, const int32_t *order, const int32_t *rowperm, const in
     constexpr uint32_t kNoRank = 0xffffffffu;
     __shared__ int64_t ts[kMaxP], te[kMaxP];
     __shared__ int hist[kMaxP + 1];
-    __shared__ int s_row, s_rstar, s_quota, s_seen;
+    __shared__ int s_row, s_rstar, s_quota, s_seen, s_next;
     const int32_t n = tc.n, P = tc.P;
     int maxc = 0;
     while (true) {
@@ -349,9 +357,10 @@ k_rows_capped(TailCtx tc, const int32_t *order, const int32_t *rowperm, const in
                     const int nw = (width + 15) >> 4 << 2;
                     for (int w = threadIdx.x; w < nw; w += blockDim.x) ctr32[w] = 0;
                     for (int o = threadIdx.x; o < width; o += blockDim.x) rank[o] = kNoRank;
+                    if (threadIdx.x == 0) s_next = 0;
                     __syncthreads();
                     const int32_t jb = (int32_t)j0;
-                    stream_chunk(tc.members, ts, te, P, jl, [&](int32_t j, int q) {
+                    stream_chunk(tc.members, ts, te, P, jl, &s_next, [&](int32_t j, int q) {
                         const int32_t o = j - jb;
                         atomicAdd(&ctr32[o >> 2], 1u << (8 * (o & 3)));
                         atomicMin(&rank[o], (uint32_t)q);
@@ -672,4 +681,58 @@ extern "C" int eacb_coassoc_fill(const int32_t *labels, int32_t n, int32_t P, in
     *host_discarded = (int64_t)dh;
     *host_max_count = mh;
     return EACB_OK;
+}
+
+// One call for the whole build: member lists, the capacity layout from the
+// largest cluster (max_assocs = factor x largest cluster when max_assocs is
+// 0, like EAC.buildMatrix, MyML/MyML/EAC/eac.py:115-140), kept counts, then
+// the rows.  indices/data hold `capacity` entries (the reference
+// preallocates the capacity layout's total, sparse.py:109-138; the kept
+// count never exceeds it); rows are written back to back (condensed).
+static size_t coassoc_build_ws(int32_t n, int32_t P, int32_t K, size_t *co, size_t *cap_ws)
+{
+    *co = (eacb_coassoc_workspace_size(n, P, K) + 255) & ~(size_t)255;
+    *cap_ws = (eacb_capacity_workspace_size(n) + 255) & ~(size_t)255;
+    return *co + *cap_ws + (((size_t)n + 1) * sizeof(int64_t) + 255) / 256 * 256;
+}
+
+extern "C" size_t eacb_coassoc_build_workspace_size(int32_t n, int32_t P, int32_t K)
+{
+    size_t co, cw;
+    return coassoc_build_ws(n, P, K, &co, &cw);
+}
+
+extern "C" int eacb_coassoc_build(const int32_t *labels, int32_t n, int32_t P, int32_t K,
+                                  int32_t cap_mode, int64_t max_assocs, int32_t factor,
+                                  int64_t *indptr, int32_t *indices, uint8_t *data,
+                                  int64_t capacity, int32_t make_diassoc, int64_t *host_nnz,
+                                  int64_t *host_discarded, int32_t *host_max_count,
+                                  int64_t *host_max_assocs, void *ws, size_t ws_bytes,
+                                  uintptr_t stream)
+{
+    if (!indptr || !indices || !data || !host_nnz || !host_discarded || !host_max_count ||
+        !host_max_assocs || !ws || (cap_mode != 0 && cap_mode != 1) || max_assocs < 0 ||
+        (max_assocs == 0 && factor <= 0) || capacity < 0)
+        return EACB_ERR_BAD_ARGUMENT;
+    size_t co, cw;
+    if (ws_bytes < coassoc_build_ws(n, P, K, &co, &cw)) return EACB_ERR_WORKSPACE;
+    char *base = (char *)ws;
+    int64_t *cap_indptr = (int64_t *)(base + co + cw);
+    int64_t maxc = 0;
+    int s = eacb_coassoc_prepare(labels, n, P, K, &maxc, base, co, stream);
+    if (s) return s;
+    const int64_t ma = max_assocs ? max_assocs : maxc * (int64_t)factor;
+    *host_max_assocs = ma;
+    if (cap_mode == 0)
+        s = eacb_capacity_linear(n, ma, 0.05, 1.0, 1.0, 0.05, cap_indptr, base + co, cw, stream);
+    else
+        s = eacb_capacity_constant(n, ma, cap_indptr, stream);
+    if (s) return s;
+    int64_t nnz = 0;
+    if ((s = eacb_coassoc_count(labels, n, P, K, cap_indptr, indptr, &nnz, base, co, stream)))
+        return s;
+    *host_nnz = nnz;
+    if (nnz > capacity) return EACB_ERR_WORKSPACE;
+    return eacb_coassoc_fill(labels, n, P, K, cap_indptr, indptr, indices, data, make_diassoc,
+                             host_discarded, host_max_count, base, co, stream);
 }

@@ -738,3 +738,105 @@ extern "C" size_t eacb_kmeans_label_workspace_size(int32_t n, int32_t d, int32_t
     TcScratch::carve(c, n, d, 1, k);
     return c.off;
 }
+
+// The label step with its arithmetic path fixed by name.
+extern "C" int eacb_kmeans_label_fp32(const float *X, int32_t n, int32_t d, const float *C,
+                                      int32_t k, int32_t *labels, float *dists, void *ws,
+                                      size_t ws_bytes, uintptr_t stream)
+{
+    return eacb_kmeans_label(X, n, d, C, k, 0, labels, dists, ws, ws_bytes, stream);
+}
+
+extern "C" int eacb_kmeans_label_bf16tc(const float *X, int32_t n, int32_t d, const float *C,
+                                        int32_t k, int32_t *labels, float *dists, void *ws,
+                                        size_t ws_bytes, uintptr_t stream)
+{
+    return eacb_kmeans_label(X, n, d, C, k, 1, labels, dists, ws, ws_bytes, stream);
+}
+
+// Workspace of one centroid update (the ensemble's second half for P = 1).
+struct CentWS {
+    int *err;
+    int32_t *kk, *active, *nempty;
+    int32_t *cnt, *members, *mypos, *args, *sel, *oarg;
+    float *key, *okey;
+    int64_t *S;
+    ScanScratch scan;
+    int64_t ntiles;
+    static CentWS carve(Carver &c, int32_t n, int32_t k)
+    {
+        CentWS w;
+        w.err = c.take<int>(1);
+        w.kk = c.take<int32_t>(1);
+        w.active = c.take<int32_t>(1);
+        w.nempty = c.take<int32_t>(1);
+        w.ntiles = ((int64_t)n + kMLTile - 1) / kMLTile;
+        const int64_t m = (int64_t)k * w.ntiles;
+        w.cnt = c.take<int32_t>(m + 1);
+        w.S = c.take<int64_t>(m + 1);
+        w.members = c.take<int32_t>(n);
+        w.mypos = c.take<int32_t>(n);
+        w.args = c.take<int32_t>(n);
+        w.sel = c.take<int32_t>(n);
+        w.oarg = c.take<int32_t>(n);
+        w.key = c.take<float>(n);
+        w.okey = c.take<float>(n);
+        w.scan = ScanScratch::carve(c, m + 1, w.err);
+        return w;
+    }
+};
+
+extern "C" size_t eacb_kmeans_centroids_workspace_size(int32_t n, int32_t d, int32_t k)
+{
+    Carver c(nullptr, 0);
+    CentWS::carve(c, n, k);
+    (void)d;
+    return c.off;
+}
+
+extern "C" int eacb_kmeans_centroids(const float *X, int32_t n, int32_t d, const int32_t *labels,
+                                     const float *dists, int32_t k, int32_t centroid_mode,
+                                     float *C, void *ws, size_t ws_bytes, uintptr_t stream)
+{
+    if (!X || n <= 0 || d <= 0 || !labels || !dists || k <= 0 || !C || !ws)
+        return EACB_ERR_BAD_ARGUMENT;
+    if (centroid_mode != 0 && centroid_mode != 1) return EACB_ERR_BAD_ARGUMENT;
+    if (d > 32 || k > 8192) return EACB_ERR_UNSUPPORTED;
+    cudaStream_t st = as_stream(stream);
+    Carver c(ws, ws_bytes);
+    CentWS w = CentWS::carve(c, n, k);
+    if (c.overflow) return EACB_ERR_WORKSPACE;
+    const int64_t nt = w.ntiles;
+    const int64_t m = (int64_t)k * nt;
+    EACB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
+    EACB_CUDA(cudaMemsetAsync(w.nempty, 0, sizeof(int32_t), st));
+    k_set2<<<1, 1, 0, st>>>(w.kk, w.active, k, 1);
+    EACB_CHECK_LAUNCH();
+    k_ml_count<<<(unsigned)nt, 256, k * sizeof(int), st>>>(labels, n, k, nt, w.cnt, w.err);
+    EACB_CHECK_LAUNCH();
+    int s = scan_launch<int32_t, int64_t>(w.cnt, w.S, m, 0, &w.S[m], w.scan, st);
+    if (s) return s;
+    const size_t place_smem = (size_t)k * (sizeof(int64_t) + sizeof(int32_t));
+    if (place_smem > 48 * 1024) EACB_CUDA(allow_max_dyn_smem(k_ml_place));
+    k_ml_place<<<(unsigned)nt, 32, place_smem, st>>>(labels, n, k, nt, w.S, w.members, w.mypos);
+    EACB_CHECK_LAUNCH();
+    const int G = 32 / d;
+    const int warps = (k + G - 1) / G;
+    dim3 cg((unsigned)((warps * 32 + 255) / 256), 1u);
+    if (centroid_mode == 1)
+        k_centroids<true><<<cg, 256, 0, st>>>(X, n, d, w.members, w.S, k, nt, w.kk, k, w.active, C,
+                                              w.nempty);
+    else
+        k_centroids<false><<<cg, 256, 0, st>>>(X, n, d, w.members, w.S, k, nt, w.kk, k, w.active, C,
+                                               w.nempty);
+    EACB_CHECK_LAUNCH();
+    // the quickselect permutes its keys: it works on a copy of the distances
+    EACB_CUDA(cudaMemcpyAsync(w.key, dists, sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    k_fill_empty<<<1, kFillThreads, 0, st>>>(X, n, d, w.key, w.S, k, nt, w.kk, k, w.active,
+                                             w.nempty, w.args, w.sel, w.okey, w.oarg, C, w.err);
+    EACB_CHECK_LAUNCH();
+    int e = 0;
+    EACB_CUDA(cudaMemcpyAsync(&e, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EACB_CUDA(cudaStreamSynchronize(st));
+    return dev_err_to_status(e);
+}
