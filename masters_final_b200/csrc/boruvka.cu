@@ -512,11 +512,15 @@ __device__ __forceinline__ bool phase_reserve(int64_t *s_cnt, unsigned long long
     return s_ok != 0;
 }
 
-// Graph rows are short (degrees): a warp takes kPhRows consecutive rows per
-// block step and stages its kept words in shared memory in one pass; the
-// block then reserves once and copies the staged words out coalesced.  A
-// warp whose staging fills up flushes it on its own (one reservation).
-constexpr int kPhRows = 16;
+// Graph rows are short (degrees), so a warp takes 32 consecutive rows per
+// block step, one row per lane for the row data.  When the 32 rows lie back
+// to back in the CSR (the usual layout), the warp walks their entries as one
+// flat range, 32 entries per step, each lane finding its entry's row among
+// the lanes' row starts (a 5-step shuffle search): the dependent loads of
+// all 32 rows overlap instead of running row after row.  Otherwise it walks
+// the rows one by one.  Kept words are staged in shared memory; the block
+// reserves once per step and copies them out coalesced (a warp whose
+// staging fills up flushes it on its own).
 constexpr int kPhStage = 512;            // staged words per warp
 
 __device__ __forceinline__ void phase_flush_warp(const uint64_t *stage, int cnt, uint64_t *eout,
@@ -534,6 +538,25 @@ __device__ __forceinline__ void phase_flush_warp(const uint64_t *stage, int cnt,
     for (int i = lane; i < cnt; i += 32) eout[b + i] = stage[i];
 }
 
+// Appends one candidate per lane to the warp's staging (flushing first when
+// it would overflow).
+__device__ __forceinline__ void phase_stage(bool keep, uint64_t k, uint64_t *stage, int &cnt,
+                                            uint64_t *eout, unsigned long long *cursor,
+                                            unsigned long long cap, int *err)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    const int nb = __popc(bal);
+    if (cnt + nb > kPhStage) {
+        __syncwarp();
+        phase_flush_warp(stage, cnt, eout, cursor, cap, err);
+        __syncwarp();
+        cnt = 0;
+    }
+    if (keep) stage[cnt + __popc(bal & ((1u << lane) - 1u))] = k;
+    cnt += nb;
+}
+
 template <typename WT>
 __global__ void __launch_bounds__(kPhThreads)
 k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const WT *weight,
@@ -545,57 +568,77 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
     __shared__ int64_t s_cnt[kPhWarps];
     __shared__ unsigned long long s_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
     uint64_t *stage = stage_all[warp];
-    const int64_t step = (int64_t)kPhWarps * kPhRows;
+    const int64_t step = (int64_t)kPhWarps * 32;
+    // entry test: the candidate word of entry e of row u (supervertex lu)
+    auto test = [&](int64_t e, int64_t u, int32_t lu, uint64_t &k) -> bool {
+        const int32_t v = dest[e];
+        if (v < 0 || v >= V) {
+            set_err(err, DEV_BAD_INPUT);
+            return false;
+        }
+        if (v == (int32_t)u) return false;
+        const uint32_t w = wword(weight[e]);
+        const int bk = (int)wbucket(w, wbits);
+        if (bk <= lo || bk > hi || label[v] == lu) return false;
+        k = pk.make(w, (uint32_t)u, (uint32_t)v);
+        return true;
+    };
     for (int64_t r0 = (int64_t)blockIdx.x * step; r0 < V; r0 += (int64_t)gridDim.x * step) {
-        const int64_t u0 = r0 + (int64_t)warp * kPhRows;
-        int cnt = 0;
-        for (int r = 0; r < kPhRows; ++r) {
-            const int64_t u = u0 + r;
-            if (u >= V) break;                       // warp-uniform
-            int64_t f = first[u], d = deg[u];
+        const int64_t u0 = r0 + (int64_t)warp * 32;
+        const int nrows = u0 >= V ? 0 : (int)(V - u0 < 32 ? V - u0 : 32);
+        int64_t f = 0, d = 0;
+        int32_t lu = 0;
+        if (lane < nrows) {
+            f = first[u0 + lane];
+            d = deg[u0 + lane];
             if (f < 0 || d < 0 || f + d > E) {
-                if (lane == 0) set_err(err, DEV_BAD_INPUT);
-                continue;
+                set_err(err, DEV_BAD_INPUT);
+                f = 0;
+                d = 0;
             }
-            const int32_t lu = label[u];
-            uint64_t m = kNone;
-            for (int64_t e0 = f; e0 < f + d; e0 += 32) {
+            lu = label[u0 + lane];
+        }
+        // rows back to back?  (row l + 1 starts where row l ends)
+        const int64_t f_next = __shfl_down_sync(0xffffffffu, f, 1);
+        const bool linked = lane + 1 >= nrows || f_next == f + d;
+        const int64_t e_begin = __shfl_sync(0xffffffffu, f, 0);
+        const int64_t e_end = nrows > 0 ? __shfl_sync(0xffffffffu, f + d, nrows - 1) : 0;
+        const bool flat = __all_sync(0xffffffffu, linked) && nrows > 0 &&
+                          e_end - e_begin < ((int64_t)1 << 30);
+        int cnt = 0;
+        if (flat) {
+            const int32_t frel = (int32_t)(f - e_begin);      // row starts, warp-relative
+            for (int64_t e0 = e_begin; e0 < e_end; e0 += 32) {
                 const int64_t e = e0 + lane;
-                bool keep = false;
-                uint64_t k = 0;
-                if (e < f + d) {
-                    const int32_t v = dest[e];
-                    if (v < 0 || v >= V) {
-                        set_err(err, DEV_BAD_INPUT);
-                    } else if (v != (int32_t)u) {
-                        const uint32_t w = wword(weight[e]);
-                        const int bk = (int)wbucket(w, wbits);
-                        if (bk > lo && bk <= hi && label[v] != lu) {
-                            keep = true;
-                            k = pk.make(w, (uint32_t)u, (uint32_t)v);
-                            m = (k >> 1) < m ? (k >> 1) : m;
-                        }
-                    }
-                }
-                const unsigned bal = __ballot_sync(0xffffffffu, keep);
-                const int nb = __popc(bal);
-                if (cnt + nb > kPhStage) {               // staging full: flush it now
-                    __syncwarp();
-                    phase_flush_warp(stage, cnt, eout, cursor, cap, err);
-                    __syncwarp();
-                    cnt = 0;
-                }
-                if (keep) stage[cnt + __popc(bal & lt)] = k;
-                cnt += nb;
-            }
+                const int32_t erel = (int32_t)(e - e_begin);
+                // row of entry e: the last row starting at or before e
+                int r = 0;
 #pragma unroll
-            for (int o = 16; o >= 1; o >>= 1) {
-                const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
-                m = x < m ? x : m;
+                for (int st = 16; st >= 1; st >>= 1) {
+                    const int c = r + st;
+                    const int32_t fs = __shfl_sync(0xffffffffu, frel, c & 31);
+                    if (c < nrows && fs <= erel) r = c;
+                }
+                const int32_t lr = __shfl_sync(0xffffffffu, lu, r);
+                uint64_t k = 0;
+                const bool keep = e < e_end && test(e, u0 + r, lr, k);
+                phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
+                if (keep) min_if_lower(&best[lr], k >> 1);
             }
-            if (lane == 0 && m != kNone) min_if_lower(&best[lu], m);
+        } else {
+            for (int rr = 0; rr < nrows; ++rr) {
+                const int64_t fr = __shfl_sync(0xffffffffu, f, rr);
+                const int64_t dr = __shfl_sync(0xffffffffu, d, rr);
+                const int32_t lr = __shfl_sync(0xffffffffu, lu, rr);
+                for (int64_t e0 = fr; e0 < fr + dr; e0 += 32) {
+                    const int64_t e = e0 + lane;
+                    uint64_t k = 0;
+                    const bool keep = e < fr + dr && test(e, u0 + rr, lr, k);
+                    phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
+                    if (keep) min_if_lower(&best[lr], k >> 1);
+                }
+            }
         }
         if (lane == 0) s_cnt[warp] = cnt;
         const bool fits = phase_reserve(s_cnt, &s_base, cursor, 1, cap, err);
@@ -883,29 +926,37 @@ __global__ void k_round_end(int64_t *cnt, int is_mst, int max_rounds, const int 
 }
 
 // MST selection key -> index of its entry in row min(u,v) of a symmetric CSR
+// (the smallest index with the key's destination and weight).  One thread
+// per key scans the row, four entries per step with their loads in flight:
+// graph rows are short, and a thread per key keeps every key's dependent
+// loads (key -> row extent -> entries) overlapping with all the others.
 template <typename WT>
 __global__ void k_key2eid(const uint64_t *keys, int64_t n_keys, const int32_t *first,
                           const int32_t *deg, const int32_t *dest, const WT *weight, Pack pk,
                           int32_t *out, int *err)
 {
-    const int lane = threadIdx.x & 31;
-    for (int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n_keys;
-         q += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        uint64_t s = keys[q];
-        int32_t a = (int32_t)pk.sel_a(s), b = (int32_t)pk.sel_b(s);
-        uint32_t w = pk.sel_w(s);
-        int64_t f = first[a], d = deg[a];
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n_keys;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t s = keys[q];
+        const int32_t a = (int32_t)pk.sel_a(s), b = (int32_t)pk.sel_b(s);
+        const uint32_t w = pk.sel_w(s);
+        const int64_t f = first[a], d = deg[a];
         int64_t found = -1;
-        for (int64_t e0 = f; e0 < f + d && found < 0; e0 += 32) {
-            int64_t e = e0 + lane;
-            bool hit = e < f + d && dest[e] == b && wword(weight[e]) == w;
-            unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (m) found = e0 + __ffs(m) - 1;
+        for (int64_t e0 = f; e0 < f + d && found < 0; e0 += 4) {
+            int32_t v[4];
+            uint32_t ww[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int64_t e = e0 + i;
+                v[i] = e < f + d ? dest[e] : -1;
+                ww[i] = e < f + d ? wword(weight[e]) : 0u;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (found < 0 && v[i] == b && ww[i] == w) found = e0 + i;
         }
-        if (lane == 0) {
-            if (found < 0) set_err(err, DEV_BAD_INPUT);   // graph not symmetric
-            out[q] = (int32_t)found;
-        }
+        if (found < 0) set_err(err, DEV_BAD_INPUT);   // graph not symmetric
+        out[q] = (int32_t)found;
     }
 }
 
@@ -1330,7 +1381,7 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
     }
     if (mode == SEL_MST) {
         if (n_mst > 0) {
-            k_key2eid<WT><<<grid_for(n_mst * 32, 256), 256, 0, st>>>(g.mst, n_mst, first, deg, dest,
+            k_key2eid<WT><<<grid_for(n_mst, 256), 256, 0, st>>>(g.mst, n_mst, first, deg, dest,
                                                                       weight, pk, mst_out, g.err);
             EACB_CHECK_LAUNCH();
         }
