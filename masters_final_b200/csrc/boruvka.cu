@@ -775,6 +775,8 @@ __global__ void k_iota(int32_t *a, int64_t n)
         a[i] = (int32_t)i;
 }
 
+constexpr int kMaxRounds = 96;   // Boruvka rounds per phase (halving: 96 is never reached)
+
 // Round state kept on the device, so that a round needs no host value and
 // the rounds can loop inside one CUDA graph (see Engine::run):
 enum : int {
@@ -787,6 +789,7 @@ enum : int {
     C_NMST = 6,       // forest edges emitted so far (all phases)
     C_ROUNDS = 7,     // rounds run in this phase
     C_DONE = 8,       // 1 once the phase has converged
+    C_ROUNDS_ALL = 9, // rounds run since the engine's reset (all phases)
     C_COUNT = 16
 };
 
@@ -893,6 +896,19 @@ __global__ void k_round_reset(unsigned long long *best, const int64_t *dV, uint6
     }
 }
 
+// Start of a phase queued without a host read: its edge count is the
+// build's cursor, its supervertex count the previous phase's result (V0
+// for the first phase).
+__global__ void k_phase_begin(int64_t *cnt, int64_t V0, int first_phase)
+{
+    if (threadIdx.x == 0) {
+        if (first_phase) cnt[C_V] = V0;
+        cnt[C_E] = cnt[C_CURSOR];
+        cnt[C_ROUNDS] = 0;
+        cnt[C_DONE] = 0;
+    }
+}
+
 __global__ void k_round_begin(int64_t *cnt, int64_t V, int64_t E)
 {
     if (threadIdx.x == 0) {
@@ -907,18 +923,23 @@ __global__ void k_round_begin(int64_t *cnt, int64_t V, int64_t E)
 // cnt[C_DONE]: 0 = continue, 1 = converged (one supervertex or no edge
 // left), 2 = no contraction (an error), 3 = round limit, 4 = device error.
 // Inside a graph, the loop condition is cleared when the phase is done.
-__global__ void k_round_end(int64_t *cnt, int is_mst, int max_rounds, const int *err,
+// A phase that stops without converging (no contraction, or the round limit
+// when that limit is not a deliberate stop) also raises DEV_CHASE_LIMIT, so
+// phases queued after it report the failure at the end.
+__global__ void k_round_end(int64_t *cnt, int is_mst, int max_rounds, int *err,
                             cudaGraphConditionalHandle h, int use_handle)
 {
     if (threadIdx.x != 0) return;
     const int64_t V = cnt[C_V], Vn = cnt[C_V_NEXT], En = cnt[C_E_NEXT];
     if (is_mst) cnt[C_NMST] += cnt[C_EMIT];
     const int64_t r = ++cnt[C_ROUNDS];
+    ++cnt[C_ROUNDS_ALL];
     int64_t done = 0;
     if (*(volatile const int *)err) done = 4;
     else if (Vn <= 1 || En == 0) done = 1;
     else if (Vn >= V) done = 2;
     else if (r >= max_rounds) done = 3;
+    if (done == 2 || (done == 3 && max_rounds >= kMaxRounds)) set_err(err, DEV_CHASE_LIMIT);
     cnt[C_DONE] = done;
     cnt[C_V] = Vn;
     cnt[C_E] = En;
@@ -976,7 +997,7 @@ struct Engine {
     int32_t V0;
     int64_t Emax;
     int64_t mst_base = 0;     // forest edges emitted by earlier phases
-    int max_rounds = 96;      // lowered only by the round-trace debug entry point
+    int max_rounds = kMaxRounds;   // lowered only by the round-trace debug entry point
 
     static Engine carve(Carver &c, int32_t V0, int64_t Emax)
     {
@@ -1025,6 +1046,12 @@ struct Engine {
     int run_phased(Pack pk, const std::vector<Phase> &plan, Build build, cudaStream_t st,
                    int64_t *n_mst_out, int64_t *n_comp_out)
     {
+        if (prof().enabled == 0 && max_rounds >= kMaxRounds) {
+            int per_round = 0;
+            cudaGraphExec_t exec = round_graph<SEL_MST>(pk, &per_round);
+            if (exec) return run_phased_graph(plan, build, exec, per_round, st, n_mst_out,
+                                              n_comp_out);
+        }
         int32_t V = V0;
         mst_base = 0;
         for (const Phase &ph : plan) {
@@ -1049,6 +1076,36 @@ struct Engine {
         }
         *n_mst_out = mst_base;
         *n_comp_out = V;
+        return EACB_OK;
+    }
+
+    // All phases queued back to back with no host read in between: a phase's
+    // edge count and supervertex count stay on the device (k_phase_begin),
+    // an empty phase runs one no-op round, and one read at the end gives the
+    // forest size, the component count and any error.
+    template <typename Build>
+    int run_phased_graph(const std::vector<Phase> &plan, Build build, cudaGraphExec_t exec,
+                         int per_round, cudaStream_t st, int64_t *n_mst_out, int64_t *n_comp_out)
+    {
+        for (size_t q = 0; q < plan.size(); ++q) {
+            EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V0, st));
+            EACB_CUDA(cudaMemsetAsync(&cnt[C_CURSOR], 0, sizeof(int64_t), st));
+            int s = build(plan[q]);
+            if (s) return s;
+            k_phase_begin<<<1, 32, 0, st>>>(cnt, V0, q == 0 ? 1 : 0);
+            EACB_CHECK_LAUNCH();
+            EACB_CUDA(cudaGraphLaunch(exec, st));
+        }
+        int64_t after[C_COUNT];
+        int e = 0;
+        EACB_CUDA(cudaMemcpyAsync(after, cnt, sizeof(after), cudaMemcpyDeviceToHost, st));
+        EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        EACB_CUDA(cudaStreamSynchronize(st));
+        count_launch((int)(after[C_ROUNDS_ALL] * per_round));
+        if (e) return dev_err_to_status(e);
+        mst_base = after[C_NMST];
+        *n_mst_out = after[C_NMST];
+        *n_comp_out = plan.empty() ? V0 : after[C_V];
         return EACB_OK;
     }
 
@@ -1171,7 +1228,7 @@ struct Engine {
         k_round_begin<<<1, 32, 0, st>>>(cnt, V_start, E0);
         EACB_CHECK_LAUNCH();
         int per_round = 0;
-        const bool host_driven = prof().enabled != 0 || max_rounds < 96;
+        const bool host_driven = prof().enabled != 0 || max_rounds < kMaxRounds;
         cudaGraphExec_t exec = host_driven ? nullptr : round_graph<MODE>(pk, &per_round);
         int64_t after[C_COUNT];
         int e = 0;
@@ -1212,7 +1269,7 @@ struct Engine {
         const int64_t done = after[C_DONE];
         if (done == 2) return EACB_ERR_NOT_CONVERGED;                 // no progress
         if (done == 0 || done == 3) {                                  // round cap
-            if (max_rounds >= 96) return EACB_ERR_NOT_CONVERGED;
+            if (max_rounds >= kMaxRounds) return EACB_ERR_NOT_CONVERGED;
         }
         *n_mst_out = after[C_NMST] - before[C_NMST];
         *n_comp_out = after[C_V];
