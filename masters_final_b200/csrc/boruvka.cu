@@ -815,8 +815,18 @@ __global__ void k_select(const unsigned long long *best, int32_t *succ, const in
     }
 }
 
+// Look-back state of the next single-pass kernel, cleared by the kernel
+// before it (one launch fewer per scan).
+__device__ __forceinline__ void clear_lookback(uint64_t *status, int64_t n_status, int *counter)
+{
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t i = t0; i < n_status; i += (int64_t)gridDim.x * blockDim.x) status[i] = 0;
+    if (t0 == 0) *counter = 0;
+}
+
 // mutual picks: the smaller id drops its edge (MyML/MyML/graph/mst.py:283-305)
-__global__ void k_mirror(const int32_t *succ, int32_t *color, int32_t *emit, const int64_t *dV)
+__global__ void k_mirror(const int32_t *succ, int32_t *color, int32_t *emit, const int64_t *dV,
+                         uint64_t *status, int64_t n_status, int *counter)
 {
     const int64_t V = *dV;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
@@ -827,28 +837,26 @@ __global__ void k_mirror(const int32_t *succ, int32_t *color, int32_t *emit, con
         color[s] = (has && !drop) ? t : (int32_t)s;
         if (emit) emit[s] = (has && !drop) ? 1 : 0;
     }
+    clear_lookback(status, n_status, counter);
 }
 
-// forest edges of this round, appended after the ones of earlier rounds
-__global__ void k_emit(const unsigned long long *best, const int32_t *emit, const int32_t *pos,
-                       uint64_t *out, const int64_t *dV, const int64_t *d_base)
+// One pass per supervertex s: (MST) emits its selected edge at its scanned
+// position, appended after the forest edges of earlier rounds; finds its root
+// by pointer chasing with path halving, bounded (a non-forest errors); flags
+// roots for the renumbering scan.  A halving step replaces c's parent p by
+// its grandparent g only if c still points at p (compare-and-swap): a plain
+// store could overwrite the root that c's own thread already stored, leaving
+// c on a non-root.  s is a root exactly when its own chase ends at s.
+__global__ void k_jump(int32_t *color, const int64_t *dV, int *err,
+                       const unsigned long long *best, int32_t *flag, const int32_t *pos,
+                       uint64_t *out, const int64_t *d_base, uint64_t *status, int64_t n_status,
+                       int *counter)
 {
     const int64_t V = *dV;
-    uint64_t *o = out + *d_base;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
-         s += (int64_t)gridDim.x * blockDim.x)
-        if (emit[s]) o[pos[s]] = best[s];
-}
-
-// roots by pointer chasing with path halving; bounded (a non-forest errors).
-// A halving step replaces c's parent p by its grandparent g only if c still
-// points at p (compare-and-swap): a plain store could overwrite the root that
-// c's own thread already stored, leaving c on a non-root.
-__global__ void k_jump(int32_t *color, const int64_t *dV, int *err)
-{
-    const int64_t V = *dV;
+    uint64_t *o = out ? out + *d_base : nullptr;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
          s += (int64_t)gridDim.x * blockDim.x) {
+        if (o && flag[s]) o[pos[s]] = best[s];
         int32_t c = color[s];
         int64_t guard = 0;
         while (true) {
@@ -863,37 +871,25 @@ __global__ void k_jump(int32_t *color, const int64_t *dV, int *err)
             }
         }
         color[s] = c;
+        flag[s] = c == (int32_t)s;
     }
+    clear_lookback(status, n_status, counter);
 }
 
-__global__ void k_rootflag(const int32_t *color, int32_t *flag, const int64_t *dV)
+// Relabels every original vertex to its new supervertex id, and clears the
+// next round's selection (Vn supervertices) and the contraction's look-back
+// state.
+__global__ void k_relabel(int32_t *label, const int32_t *color, const int32_t *newid, int64_t V0,
+                          unsigned long long *best, const int64_t *dVn, uint64_t *status,
+                          int64_t n_status, int *counter, int64_t *d_count)
 {
-    const int64_t V = *dV;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
-         s += (int64_t)gridDim.x * blockDim.x)
-        flag[s] = color[s] == (int32_t)s;
-}
-
-__global__ void k_relabel(int32_t *label, const int32_t *color, const int32_t *newid, int64_t V0)
-{
-    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < V0;
-         x += (int64_t)gridDim.x * blockDim.x)
-        label[x] = newid[color[label[x]]];
-}
-
-// Clears the next round's selection and the contraction's look-back state.
-__global__ void k_round_reset(unsigned long long *best, const int64_t *dV, uint64_t *status,
-                              int64_t n_status, int *counter, int64_t *d_count)
-{
-    const int64_t V = *dV;
+    const int64_t Vn = *dVn;
     const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t s = t0; s < V; s += stride) best[s] = kNone;
-    for (int64_t s = t0; s < n_status; s += stride) status[s] = 0;
-    if (t0 == 0) {
-        *counter = 0;
-        *d_count = 0;
-    }
+    for (int64_t x = t0; x < V0; x += stride) label[x] = newid[color[label[x]]];
+    for (int64_t x = t0; x < Vn; x += stride) best[x] = kNone;
+    clear_lookback(status, n_status, counter);
+    if (t0 == 0) *d_count = 0;
 }
 
 // Start of a phase queued without a host read: its edge count is the
@@ -1152,34 +1148,33 @@ struct Engine {
     {
         const unsigned gv = 296;
         int launches = 0;
+        // look-back status words: scans over V0, the contraction over Emax
+        const int64_t vtiles = (V0 + kScanTile - 1) / kScanTile;
+        const int64_t etiles = (Emax + kETile - 1) / kETile;
         k_select<MODE><<<gv, 256, 0, st>>>(best, succ, &cnt[C_V], label, pk);
         EACB_CHECK_LAUNCH();
-        k_mirror<<<gv, 256, 0, st>>>(succ, color, MODE == SEL_MST ? flag : nullptr, &cnt[C_V]);
+        k_mirror<<<gv, 256, 0, st>>>(succ, color, MODE == SEL_MST ? flag : nullptr, &cnt[C_V],
+                                     scan.status, vtiles, scan.counter);
         EACB_CHECK_LAUNCH();
         launches += 2;
         if (MODE == SEL_MST) {
             int s = scan_launch_dev<int32_t, int32_t>(flag, pos, &cnt[C_V], V0, 0, &cnt[C_EMIT],
-                                                      scan, st);
+                                                      scan, st, false);
             if (s) return s;
-            k_emit<<<gv, 256, 0, st>>>(best, flag, pos, mst, &cnt[C_V], &cnt[C_NMST]);
-            EACB_CHECK_LAUNCH();
-            launches += 3;
+            launches += 1;
         }
-        k_jump<<<gv, 256, 0, st>>>(color, &cnt[C_V], err);
-        EACB_CHECK_LAUNCH();
-        k_rootflag<<<gv, 256, 0, st>>>(color, flag, &cnt[C_V]);
+        k_jump<<<gv, 256, 0, st>>>(color, &cnt[C_V], err, best, flag, pos,
+                                   MODE == SEL_MST ? mst : nullptr, &cnt[C_NMST], scan.status,
+                                   vtiles, scan.counter);
         EACB_CHECK_LAUNCH();
         int s = scan_launch_dev<int32_t, int32_t>(flag, pos, &cnt[C_V], V0, 0, &cnt[C_V_NEXT],
-                                                  scan, st);
+                                                  scan, st, false);
         if (s) return s;
-        k_relabel<<<grid_for(V0, 256), 256, 0, st>>>(label, color, pos, V0);
+        k_relabel<<<grid_for(V0, 256), 256, 0, st>>>(label, color, pos, V0, best, &cnt[C_V_NEXT],
+                                                       scan.status, etiles > 0 ? etiles : 1,
+                                                       scan.counter, &cnt[C_E_NEXT]);
         EACB_CHECK_LAUNCH();
-        const int64_t etiles = (Emax + kETile - 1) / kETile;
-        k_round_reset<<<grid_for(V0, 256), 256, 0, st>>>(best, &cnt[C_V_NEXT], scan.status,
-                                                           etiles > 0 ? etiles : 1, scan.counter,
-                                                           &cnt[C_E_NEXT]);
-        EACB_CHECK_LAUNCH();
-        launches += 6;
+        launches += 3;
         cudaEvent_t ev0 = nullptr, ev1 = nullptr;
         if (timed_filter) {
             cudaEventCreate(&ev0);

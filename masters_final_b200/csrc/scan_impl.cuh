@@ -108,15 +108,20 @@ __global__ void k_set_i64(int64_t *p, int64_t v);
 __global__ void k_clear_status(uint64_t *status, int64_t n, int *counter);
 
 // Scan whose length is read on the device (*d_n <= max_n); no memset calls,
-// so it can be captured into a conditional graph body.
+// so it can be captured into a conditional graph body.  With clear = false
+// the caller's previous kernel has already zeroed the look-back state
+// (status words [0, ceil(max_n / kScanTile)) and the tile counter).
 template <typename TIn, typename TOut>
 inline int scan_launch_dev(const TIn *in, TOut *out, const int64_t *d_n, int64_t max_n,
-                           int64_t init, int64_t *d_total, const ScanScratch &s, cudaStream_t st)
+                           int64_t init, int64_t *d_total, const ScanScratch &s, cudaStream_t st,
+                           bool clear = true)
 {
     const int64_t ntiles = (max_n + kScanTile - 1) / kScanTile;
     const int64_t grid = ntiles > 0 ? ntiles : 1;
-    k_clear_status<<<grid_for(grid, 256, 148 * 4), 256, 0, st>>>(s.status, grid, s.counter);
-    EACB_CHECK_LAUNCH();
+    if (clear) {
+        k_clear_status<<<grid_for(grid, 256, 148 * 4), 256, 0, st>>>(s.status, grid, s.counter);
+        EACB_CHECK_LAUNCH();
+    }
     if (((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0))
         k_scan<TIn, TOut, true><<<(unsigned)grid, kScanThreads, 0, st>>>(
             in, out, max_n, init, s.status, s.counter, d_total, s.err, d_n);
