@@ -560,10 +560,14 @@ __device__ __forceinline__ void phase_stage(bool keep, uint64_t k, uint64_t *sta
 template <typename WT>
 __global__ void __launch_bounds__(kPhThreads)
 k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const WT *weight,
-            int32_t V, int64_t E, int wbits, int lo, int hi, const int32_t *label, Pack pk,
-            uint64_t *eout, unsigned long long *cursor, unsigned long long cap,
-            unsigned long long *best, int *err)
+            int32_t V, int64_t E, int wbits, int lo, int hi, const int *dev_lohi, int slot,
+            const int32_t *label, Pack pk, uint64_t *eout, unsigned long long *cursor,
+            unsigned long long cap, unsigned long long *best, int *err)
 {
+    if (dev_lohi) {
+        lo = dev_lohi[2 * slot];
+        hi = dev_lohi[2 * slot + 1];
+    }
     __shared__ uint64_t stage_all[kPhWarps][kPhStage];
     __shared__ int64_t s_cnt[kPhWarps];
     __shared__ unsigned long long s_base;
@@ -730,16 +734,18 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
     }
 }
 
-// One phase: the entries with weight bucket in (lo, hi] of rows [r0, r1).
+// One phase: the entries with weight bucket in (lo, hi] of rows [r0, r1);
+// with slot >= 0 the range is read on the device from the plan's slot.
 struct Phase {
     int lo, hi;
     int64_t r0, r1;
+    int slot;
 };
 
 // Phase ranges (lo, hi] of weight buckets: cut the bucket histogram at the
 // given cumulative fractions of the entries.
-static int phase_ranges(const unsigned long long *hist, const double *fracs, int nf, int *lo,
-                        int *hi)
+__host__ __device__ static int phase_ranges(const unsigned long long *hist, const double *fracs,
+                                            int nf, int *lo, int *hi)
 {
     unsigned long long tot = 0;
     for (int b = 0; b < 256; ++b) tot += hist[b];
@@ -766,6 +772,22 @@ static int phase_ranges(const unsigned long long *hist, const double *fracs, int
         np++;
     }
     return np;
+}
+
+// The weight phases of an MST on the device (no host read): ranges (lo, hi]
+// at cumulative fractions 1/8, 1/2, 1 of the histogram, one slot each in
+// lohi (an unused slot holds the empty range (255, 255]).
+constexpr int kPhaseSlots = 3;
+__global__ void k_phase_plan(const unsigned long long *hist, int *lohi)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double fracs[kPhaseSlots] = {0.125, 0.5, 1.0};
+    int lo[8], hi[8];
+    const int np = phase_ranges(hist, fracs, kPhaseSlots, lo, hi);
+    for (int q = 0; q < kPhaseSlots; ++q) {
+        lohi[2 * q] = q < np ? lo[q] : 255;
+        lohi[2 * q + 1] = q < np ? hi[q] : 255;
+    }
 }
 
 __global__ void k_iota(int32_t *a, int64_t n)
@@ -989,6 +1011,7 @@ struct Engine {
     int32_t *succ, *color, *flag, *pos;
     uint64_t *mst;
     unsigned long long *hist; // 256 weight buckets
+    int *lohi;                // the device phase plan (k_phase_plan)
     ScanScratch scan;
     int32_t V0;
     int64_t Emax;
@@ -1001,6 +1024,7 @@ struct Engine {
         g.err = c.take<int>(1);
         g.cnt = c.take<int64_t>(C_COUNT);
         g.hist = c.take<unsigned long long>(256);
+        g.lohi = c.take<int>(2 * kPhaseSlots);
         g.V0 = V0;
         g.Emax = Emax;
         // one edge array (contraction is in place); eb holds the two
@@ -1392,19 +1416,18 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
             }
             EACB_CHECK_LAUNCH();
         }
-        unsigned long long h[256];
-        if ((s = g.read_hist(st, h))) return s;
-        const double fracs[3] = {0.125, 0.5, 1.0};
-        int lo[8], hi[8];
-        const int np = phase_ranges(h, fracs, 3, lo, hi);
+        // the phase plan stays on the device: the whole MST is queued without
+        // a host read until its end
+        k_phase_plan<<<1, 32, 0, st>>>(g.hist, g.lohi);
+        EACB_CHECK_LAUNCH();
         std::vector<Phase> plan;
-        for (int q = 0; q < np; ++q) plan.push_back(Phase{lo[q], hi[q], 0, V});
+        for (int q = 0; q < kPhaseSlots; ++q) plan.push_back(Phase{0, 0, 0, V, q});
         // a phase holds a subset of the E entries: the edge array always fits
         auto build = [&](const Phase &ph) -> int {
             if (E == 0) return EACB_OK;
             ProfScope ps(PROF_PHASE, st);
             k_phase_csr<WT><<<gr, kPhThreads, 0, st>>>(
-                first, deg, dest, weight, V, E, wbits, ph.lo, ph.hi, g.label, pk, g.ea,
+                first, deg, dest, weight, V, E, wbits, 0, 0, g.lohi, ph.slot, g.label, pk, g.ea,
                 (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best,
                 g.err);
             EACB_CHECK_LAUNCH();
@@ -1658,7 +1681,7 @@ static int plan_final_phases(const unsigned long long h[256], int64_t cap_entrie
                 acc += h[b];
                 continue;
             }
-            if (acc) plan.push_back(Phase{start, b - 1, 0, n});
+            if (acc) plan.push_back(Phase{start, b - 1, 0, n, -1});
             start = b - 1;
             acc = 0;
             if (h[b] <= (unsigned long long)cap_entries) {
@@ -1676,12 +1699,12 @@ static int plan_final_phases(const unsigned long long h[256], int64_t cap_entrie
             while (r0 < n) {
                 int64_t r1 = r0 + 1;
                 while (r1 < n && ip[r1 + 1] - ip[r0] <= cap_entries) ++r1;
-                plan.push_back(Phase{b - 1, b, r0, r1});
+                plan.push_back(Phase{b - 1, b, r0, r1, -1});
                 r0 = r1;
             }
             start = b;
         }
-        if (acc) plan.push_back(Phase{start, hi[q], 0, n});
+        if (acc) plan.push_back(Phase{start, hi[q], 0, n, -1});
     }
     return EACB_OK;
 }
