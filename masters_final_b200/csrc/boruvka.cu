@@ -613,22 +613,55 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
         int cnt = 0;
         if (flat) {
             const int32_t frel = (int32_t)(f - e_begin);      // row starts, warp-relative
-            for (int64_t e0 = e_begin; e0 < e_end; e0 += 32) {
-                const int64_t e = e0 + lane;
-                const int32_t erel = (int32_t)(e - e_begin);
-                // row of entry e: the last row starting at or before e
-                int r = 0;
+            // two 32-entry slices per step, the loads of both in flight together
+            constexpr int S = 2;
+            for (int64_t e0 = e_begin; e0 < e_end; e0 += 32 * S) {
+                int64_t e[S];
+                int r[S];
+                int32_t lr[S], v[S];
+                uint32_t w[S];
+                bool in[S];
 #pragma unroll
-                for (int st = 16; st >= 1; st >>= 1) {
-                    const int c = r + st;
-                    const int32_t fs = __shfl_sync(0xffffffffu, frel, c & 31);
-                    if (c < nrows && fs <= erel) r = c;
+                for (int q = 0; q < S; ++q) {
+                    e[q] = e0 + 32 * q + lane;
+                    in[q] = e[q] < e_end;
+                    const int32_t erel = (int32_t)(e[q] - e_begin);
+                    // row of entry e: the last row starting at or before e
+                    int rr = 0;
+#pragma unroll
+                    for (int st = 16; st >= 1; st >>= 1) {
+                        const int c = rr + st;
+                        const int32_t fs = __shfl_sync(0xffffffffu, frel, c & 31);
+                        if (c < nrows && fs <= erel) rr = c;
+                    }
+                    r[q] = rr;
+                    lr[q] = __shfl_sync(0xffffffffu, lu, rr);
+                    v[q] = in[q] ? dest[e[q]] : -1;
+                    w[q] = in[q] ? wword(weight[e[q]]) : 0u;
                 }
-                const int32_t lr = __shfl_sync(0xffffffffu, lu, r);
-                uint64_t k = 0;
-                const bool keep = e < e_end && test(e, u0 + r, lr, k);
-                phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
-                if (keep) min_if_lower(&best[lr], k >> 1);
+                bool cand[S];
+                int32_t lv[S];
+#pragma unroll
+                for (int q = 0; q < S; ++q) {
+                    cand[q] = false;
+                    if (in[q]) {
+                        if (v[q] < 0 || v[q] >= V) {
+                            set_err(err, DEV_BAD_INPUT);
+                        } else if (v[q] != (int32_t)(u0 + r[q])) {
+                            const int bk = (int)wbucket(w[q], wbits);
+                            cand[q] = bk > lo && bk <= hi;
+                        }
+                    }
+                    lv[q] = cand[q] ? label[v[q]] : 0;
+                }
+#pragma unroll
+                for (int q = 0; q < S; ++q) {
+                    const bool keep = cand[q] && lv[q] != lr[q];
+                    const uint64_t k =
+                        keep ? pk.make(w[q], (uint32_t)(u0 + r[q]), (uint32_t)v[q]) : 0ull;
+                    phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
+                    if (keep) min_if_lower(&best[lr[q]], k >> 1);
+                }
             }
         } else {
             for (int rr = 0; rr < nrows; ++rr) {
