@@ -613,8 +613,8 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
         int cnt = 0;
         if (flat) {
             const int32_t frel = (int32_t)(f - e_begin);      // row starts, warp-relative
-            // two 32-entry slices per step, the loads of both in flight together
-            constexpr int S = 2;
+            // four 32-entry slices per step, the loads of all in flight together
+            constexpr int S = 4;
             for (int64_t e0 = e_begin; e0 < e_end; e0 += 32 * S) {
                 int64_t e[S];
                 int r[S];
