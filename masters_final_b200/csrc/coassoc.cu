@@ -40,7 +40,11 @@ namespace eacb {
 constexpr int kMaxK = 8192;            // largest cluster id + 1 supported
 constexpr int kRowThreads = 512;
 constexpr int kBitmapBytes = 96 * 1024;        // pass 1: 786,432 columns per chunk
-constexpr int kCountBytes = 96 * 1024;         // pass 2: 98,304 columns per chunk
+// pass 2 runs one 1024-thread CTA per SM with ~208 KB of byte counters:
+// rows of large n span many column chunks, and each chunk costs a walk step
+// per tail plus a clear and a compaction whatever its width
+constexpr int kFillThreads = 1024;
+constexpr int kCountBytes = 208 * 1024;        // pass 2: 212,992 columns per chunk
 constexpr int kCapCols = 16 * 1024;            // capped rows: columns per chunk
 constexpr int kCapSmem = kCapCols * 5;         // byte counters + 32-bit ranks
 constexpr int kMaxP = 255;
@@ -213,51 +217,51 @@ k_rows_count(TailCtx tc, const int32_t *order, const int32_t *rowperm, const int
 
 // ---------------------------------------------------------------- pass 2 --
 // Block-wide ordered compaction of the non-zero byte counters of a chunk.
-// Each thread owns a contiguous 16-byte-aligned segment.
-template <typename Keep>
+// Each thread owns a contiguous 16-byte-aligned segment.  A row of a large
+// matrix spans many more columns than it keeps, so most 16-byte vectors are
+// zero: they cost one OR each, and a non-zero vector's kept bytes are found
+// with a per-byte compare mask (counters past `width` are zero: the chunk is
+// cleared in whole vectors and only columns below it are counted).
+template <int THREADS>
 __device__ __forceinline__ int64_t emit_chunk(const uint8_t *ctr, int width, int32_t jb,
                                               int32_t *indices, uint8_t *data, int64_t out0,
-                                              Keep keep, int &maxc)
+                                              int &maxc)
 {
     const int nvec = (width + 15) >> 4;
     const int per = (nvec + blockDim.x - 1) / blockDim.x;
     const int v0 = threadIdx.x * per, v1 = min(nvec, v0 + per);
+    const uint4 *cv = reinterpret_cast<const uint4 *>(ctr);
     int mine = 0;
     for (int v = v0; v < v1; ++v) {
-        uint4 x = reinterpret_cast<const uint4 *>(ctr)[v];
-        const uint32_t w4[4] = {x.x, x.y, x.z, x.w};
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int o = v * 16 + q * 4 + b;
-                const uint32_t cnt = (w4[q] >> (8 * b)) & 255u;
-                if (cnt && o < width && keep(o, cnt)) mine++;
-            }
+        const uint4 x = cv[v];
+        if ((x.x | x.y | x.z | x.w) == 0u) continue;
+        mine += (__popc(__vcmpne4(x.x, 0u)) + __popc(__vcmpne4(x.y, 0u)) +
+                 __popc(__vcmpne4(x.z, 0u)) + __popc(__vcmpne4(x.w, 0u))) >> 3;
     }
     int64_t tot;
-    int64_t at = out0 + block_excl_sum<kRowThreads>(mine, tot);
+    int64_t at = out0 + block_excl_sum<THREADS>(mine, tot);
     for (int v = v0; v < v1; ++v) {
-        uint4 x = reinterpret_cast<const uint4 *>(ctr)[v];
+        const uint4 x = cv[v];
+        if ((x.x | x.y | x.z | x.w) == 0u) continue;
         const uint32_t w4[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int o = v * 16 + q * 4 + b;
-                const uint32_t cnt = (w4[q] >> (8 * b)) & 255u;
-                if (cnt && o < width && keep(o, cnt)) {
-                    indices[at] = jb + o;
-                    data[at] = (uint8_t)cnt;
-                    maxc = max(maxc, (int)cnt);
-                    at++;
-                }
+        for (int q = 0; q < 4; ++q) {
+            uint32_t m = __vcmpne4(w4[q], 0u);       // 0xff in each non-zero byte
+            while (m) {
+                const int bb = (__ffs(m) - 1) >> 3;
+                m &= ~(0xffu << (8 * bb));
+                const uint32_t cnt = (w4[q] >> (8 * bb)) & 255u;
+                indices[at] = jb + v * 16 + q * 4 + bb;
+                data[at] = (uint8_t)cnt;
+                maxc = max(maxc, (int)cnt);
+                at++;
             }
+        }
     }
     return tot;
 }
 
-__global__ void __launch_bounds__(kRowThreads)
+__global__ void __launch_bounds__(kFillThreads)
 k_rows_fill(TailCtx tc, const int32_t *rowperm, const int32_t *rowflag, const int64_t *indptr,
             int32_t *indices, uint8_t *data, int *queue, int *gmax, int *err)
 {
@@ -293,8 +297,8 @@ k_rows_fill(TailCtx tc, const int32_t *rowperm, const int32_t *rowflag, const in
                 atomicAdd(&ctr32[o >> 2], 1u << (8 * (o & 3)));
             });
             __syncthreads();
-            out += emit_chunk((const uint8_t *)ctr32, width, jb, indices, data, out,
-                              [](int, uint32_t) { return true; }, maxc);
+            out += emit_chunk<kFillThreads>((const uint8_t *)ctr32, width, jb, indices, data, out,
+                                            maxc);
             __syncthreads();
         }
         if (threadIdx.x == 0 && out != indptr[i + 1]) set_err(err, DEV_CAPACITY);
@@ -487,12 +491,12 @@ static int read_err(int *err, cudaStream_t st)
     return dev_err_to_status(e);
 }
 
-static int row_grid()
+static int row_grid(int ctas_per_sm = 2)
 {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return 2 * sms;
+    return ctas_per_sm * sms;
 }
 
 }  // namespace eacb
@@ -659,7 +663,7 @@ extern "C" int eacb_coassoc_fill(const int32_t *labels, int32_t n, int32_t P, in
     EACB_CUDA(allow_max_dyn_smem(k_rows_fill));
     EACB_CUDA(allow_max_dyn_smem(k_rows_capped));
     ProfScope ps(PROF_COASSOC, st);
-    k_rows_fill<<<row_grid(), kRowThreads, kCountBytes, st>>>(
+    k_rows_fill<<<row_grid(1), kFillThreads, kCountBytes, st>>>(
         tc, w.rowperm, w.rowflag, indptr, indices, data, &w.queue[1], w.maxcnt, w.err);
     EACB_CHECK_LAUNCH();
     ps.done(0.0);
