@@ -40,11 +40,15 @@ namespace eacb {
 constexpr int kMaxK = 8192;            // largest cluster id + 1 supported
 constexpr int kRowThreads = 512;
 constexpr int kBitmapBytes = 96 * 1024;        // pass 1: 786,432 columns per chunk
-// pass 2 runs one 1024-thread CTA per SM with ~208 KB of byte counters:
-// rows of large n span many column chunks, and each chunk costs a walk step
-// per tail plus a clear and a compaction whatever its width
+// pass 2 runs one 1024-thread CTA per SM with 192 KB of byte counters and a
+// "touched" flag byte per 16 counters: rows of large n span many column
+// chunks, and each chunk costs a walk step per tail; the compaction reads
+// only flagged counter vectors and clears what it reads, so a chunk costs no
+// pass over its mostly-zero counters
 constexpr int kFillThreads = 1024;
-constexpr int kCountBytes = 208 * 1024;        // pass 2: 212,992 columns per chunk
+constexpr int kFillVecs = 12;                  // counter vectors (16 columns) per thread
+constexpr int kCountBytes = kFillThreads * kFillVecs * 16;   // 196,608 columns per chunk
+constexpr int kFillSmem = kCountBytes + kCountBytes / 16;
 constexpr int kCapCols = 16 * 1024;            // capped rows: columns per chunk
 constexpr int kCapSmem = kCapCols * 5;         // byte counters + 32-bit ranks
 constexpr int kMaxP = 255;
@@ -121,7 +125,7 @@ template <int THREADS>
 __device__ __forceinline__ int64_t block_sum(int64_t v)
 {
     int64_t tot;
-    block_excl_sum<THREADS>(v, tot);
+    block_excl_sum_shfl<THREADS>(v, tot);
     return tot;
 }
 
@@ -193,8 +197,9 @@ k_rows_count(TailCtx tc, const int32_t *order, const int32_t *rowperm, const int
         int64_t D = 0;
         for (int64_t j0 = (int64_t)i + 1; j0 < n; j0 += kCols) {
             const int32_t jl = (int32_t)((j0 + kCols < n) ? j0 + kCols : n);
-            const int nwords = (int)((jl - j0 + 31) >> 5);
-            for (int w = threadIdx.x; w < nwords; w += blockDim.x) bm[w] = 0;
+            const int nvec = (int)((jl - j0 + 127) >> 7);      // 128 columns per vector
+            uint4 *b4 = reinterpret_cast<uint4 *>(bm);
+            for (int w = threadIdx.x; w < nvec; w += blockDim.x) b4[w] = make_uint4(0u, 0u, 0u, 0u);
             if (threadIdx.x == 0) s_next = 0;
             __syncthreads();
             const int32_t jb = (int32_t)j0;
@@ -204,7 +209,10 @@ k_rows_count(TailCtx tc, const int32_t *order, const int32_t *rowperm, const int
             });
             __syncthreads();
             int64_t c = 0;
-            for (int w = threadIdx.x; w < nwords; w += blockDim.x) c += __popc(bm[w]);
+            for (int w = threadIdx.x; w < nvec; w += blockDim.x) {
+                const uint4 x = b4[w];
+                c += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+            }
             D += block_sum<kRowThreads>(c);
         }
         if (threadIdx.x == 0) {
@@ -216,34 +224,38 @@ k_rows_count(TailCtx tc, const int32_t *order, const int32_t *rowperm, const int
 }
 
 // ---------------------------------------------------------------- pass 2 --
-// Block-wide ordered compaction of the non-zero byte counters of a chunk.
-// Each thread owns a contiguous 16-byte-aligned segment.  A row of a large
-// matrix spans many more columns than it keeps, so most 16-byte vectors are
-// zero: they cost one OR each, and a non-zero vector's kept bytes are found
-// with a per-byte compare mask (counters past `width` are zero: the chunk is
-// cleared in whole vectors and only columns below it are counted).
-template <int THREADS>
-__device__ __forceinline__ int64_t emit_chunk(const uint8_t *ctr, int width, int32_t jb,
-                                              int32_t *indices, uint8_t *data, int64_t out0,
-                                              int &maxc)
+// Block-wide ordered compaction of a chunk's non-zero byte counters.  Thread
+// t owns counter vectors [kFillVecs t, kFillVecs (t + 1)) (16 columns each)
+// and their flag bytes (kFillVecs / 4 words); it counts the kept bytes of its
+// flagged vectors with per-byte compare masks, places them after a block
+// scan, writes them in column order and clears the vectors and flags.
+__device__ __forceinline__ int64_t emit_flagged(uint32_t *ctr32, uint32_t *flag32, int32_t jb,
+                                                int32_t *indices, uint8_t *data, int64_t out0,
+                                                int &maxc)
 {
-    const int nvec = (width + 15) >> 4;
-    const int per = (nvec + blockDim.x - 1) / blockDim.x;
-    const int v0 = threadIdx.x * per, v1 = min(nvec, v0 + per);
-    const uint4 *cv = reinterpret_cast<const uint4 *>(ctr);
+    static_assert(kFillVecs % 4 == 0, "a thread's flags are whole words");
+    uint32_t *fw = flag32 + threadIdx.x * (kFillVecs / 4);
+    uint4 *cv = reinterpret_cast<uint4 *>(ctr32) + threadIdx.x * kFillVecs;
+    uint32_t fm = 0;                                   // bit q: vector q flagged
+#pragma unroll
+    for (int k = 0; k < kFillVecs / 4; ++k) {
+        const uint32_t m = __vcmpne4(fw[k], 0u);
+        fm |= (((m >> 7) & 1u) | ((m >> 14) & 2u) | ((m >> 21) & 4u) | ((m >> 28) & 8u)) << (4 * k);
+    }
     int mine = 0;
-    for (int v = v0; v < v1; ++v) {
-        const uint4 x = cv[v];
-        if ((x.x | x.y | x.z | x.w) == 0u) continue;
+    for (uint32_t b = fm; b; b &= b - 1u) {
+        const uint4 x = cv[__ffs(b) - 1];
         mine += (__popc(__vcmpne4(x.x, 0u)) + __popc(__vcmpne4(x.y, 0u)) +
                  __popc(__vcmpne4(x.z, 0u)) + __popc(__vcmpne4(x.w, 0u))) >> 3;
     }
     int64_t tot;
-    int64_t at = out0 + block_excl_sum<THREADS>(mine, tot);
-    for (int v = v0; v < v1; ++v) {
+    int64_t at = out0 + block_excl_sum_shfl<kFillThreads>(mine, tot);
+    for (uint32_t b = fm; b; b &= b - 1u) {
+        const int v = __ffs(b) - 1;
         const uint4 x = cv[v];
-        if ((x.x | x.y | x.z | x.w) == 0u) continue;
+        cv[v] = make_uint4(0u, 0u, 0u, 0u);
         const uint32_t w4[4] = {x.x, x.y, x.z, x.w};
+        const int32_t c0 = jb + (int32_t)(threadIdx.x * kFillVecs + v) * 16;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             uint32_t m = __vcmpne4(w4[q], 0u);       // 0xff in each non-zero byte
@@ -251,26 +263,35 @@ __device__ __forceinline__ int64_t emit_chunk(const uint8_t *ctr, int width, int
                 const int bb = (__ffs(m) - 1) >> 3;
                 m &= ~(0xffu << (8 * bb));
                 const uint32_t cnt = (w4[q] >> (8 * bb)) & 255u;
-                indices[at] = jb + v * 16 + q * 4 + bb;
+                indices[at] = c0 + q * 4 + bb;
                 data[at] = (uint8_t)cnt;
                 maxc = max(maxc, (int)cnt);
                 at++;
             }
         }
     }
+    if (fm) {
+#pragma unroll
+        for (int k = 0; k < kFillVecs / 4; ++k) fw[k] = 0u;
+    }
     return tot;
 }
 
-__global__ void __launch_bounds__(kFillThreads)
+__global__ void __launch_bounds__(kFillThreads, 1)
 k_rows_fill(TailCtx tc, const int32_t *rowperm, const int32_t *rowflag, const int64_t *indptr,
             int32_t *indices, uint8_t *data, int *queue, int *gmax, int *err)
 {
     extern __shared__ uint32_t ctr32[];
+    uint32_t *flag32 = ctr32 + kCountBytes / 4;
+    uint8_t *flag = reinterpret_cast<uint8_t *>(flag32);
     __shared__ int64_t ts[kMaxP], te[kMaxP];
     __shared__ int s_row, s_next;
     const int32_t n = tc.n, P = tc.P;
     constexpr int32_t kCols = kCountBytes;
     int maxc = 0;
+    // counters and flags start at zero; each compaction clears what it read
+    for (int w = threadIdx.x; w < kFillSmem / 16; w += blockDim.x)
+        reinterpret_cast<uint4 *>(ctr32)[w] = make_uint4(0u, 0u, 0u, 0u);
     while (true) {
         const int qi = next_row(queue, &s_row);
         if (qi >= n) break;
@@ -282,24 +303,19 @@ k_rows_fill(TailCtx tc, const int32_t *rowperm, const int32_t *rowflag, const in
             ts[p] = s;
             te[p] = e;
         }
-        __syncthreads();
         int64_t out = indptr[i];
         for (int64_t j0 = (int64_t)i + 1; j0 < n; j0 += kCols) {
             const int32_t jl = (int32_t)((j0 + kCols < n) ? j0 + kCols : n);
-            const int width = (int)(jl - j0);
-            const int nwords = (width + 15) >> 4 << 2;
-            for (int w = threadIdx.x; w < nwords; w += blockDim.x) ctr32[w] = 0;
             if (threadIdx.x == 0) s_next = 0;
             __syncthreads();
             const int32_t jb = (int32_t)j0;
             stream_chunk(tc.members, ts, te, P, jl, &s_next, [&](int32_t j, int) {
                 const int32_t o = j - jb;
                 atomicAdd(&ctr32[o >> 2], 1u << (8 * (o & 3)));
+                flag[o >> 4] = 1;
             });
             __syncthreads();
-            out += emit_chunk<kFillThreads>((const uint8_t *)ctr32, width, jb, indices, data, out,
-                                            maxc);
-            __syncthreads();
+            out += emit_flagged(ctr32, flag32, jb, indices, data, out, maxc);
         }
         if (threadIdx.x == 0 && out != indptr[i + 1]) set_err(err, DEV_CAPACITY);
     }
@@ -663,7 +679,7 @@ extern "C" int eacb_coassoc_fill(const int32_t *labels, int32_t n, int32_t P, in
     EACB_CUDA(allow_max_dyn_smem(k_rows_fill));
     EACB_CUDA(allow_max_dyn_smem(k_rows_capped));
     ProfScope ps(PROF_COASSOC, st);
-    k_rows_fill<<<row_grid(1), kFillThreads, kCountBytes, st>>>(
+    k_rows_fill<<<row_grid(1), kFillThreads, kFillSmem, st>>>(
         tc, w.rowperm, w.rowflag, indptr, indices, data, &w.queue[1], w.maxcnt, w.err);
     EACB_CHECK_LAUNCH();
     ps.done(0.0);

@@ -169,6 +169,32 @@ __device__ __forceinline__ int64_t block_excl_sum(int64_t v, int64_t &total)
     return r;
 }
 
+// The same result with the warp totals combined by warp 0 in shuffles (three
+// barriers, no serial steps): for the row kernels, which scan once per
+// column chunk.
+template <int THREADS>
+__device__ __forceinline__ int64_t block_excl_sum_shfl(int64_t v, int64_t &total)
+{
+    constexpr int W = THREADS / 32;
+    static_assert(W >= 1 && W <= 32, "one warp combines the warp totals");
+    __shared__ int64_t wpre[W + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t inc = warp_incl_sum(v);
+    if (lane == 31) wpre[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int64_t x = lane < W ? wpre[lane] : 0;
+        const int64_t xi = warp_incl_sum(x);
+        if (lane < W) wpre[lane] = xi - x;
+        if (lane == 31) wpre[W] = xi;
+    }
+    __syncthreads();
+    const int64_t r = wpre[warp] + inc - v;
+    total = wpre[W];
+    __syncthreads();                 // wpre is rewritten by the next call
+    return r;
+}
+
 // ---------------------------------------------------------------------------
 // Decoupled look-back (single-pass scan across tiles).  One 64-bit status word
 // per tile: bits 63..62 = flag (0 empty, 1 aggregate, 2 inclusive prefix),

@@ -368,7 +368,7 @@ __device__ __forceinline__ int64_t count_le(const int32_t *a, int64_t len, int64
     return lo;
 }
 
-__global__ void __launch_bounds__(kFillThreads)
+__global__ void __launch_bounds__(kFillThreads, 1)
 k_fill_empty(const float *X, int32_t n, int32_t D, float *dists, const int64_t *S, int32_t K,
              int64_t ntiles, const int32_t *kk, int32_t kmax, const int32_t *active,
              const int32_t *nempty, int32_t *args_all, int32_t *sel_all, float *okey_all,
