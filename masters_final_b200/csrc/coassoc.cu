@@ -151,19 +151,23 @@ __device__ __forceinline__ void stream_chunk(const int32_t *members, int64_t *ts
         int64_t cur = ts[p];
         const int64_t end = te[p];
         while (cur < end) {
+            // 32-bit offsets from the step's base keep the per-member work to
+            // a compare, a load and the op; the count taken is one reduction
+            const int32_t *base = members + cur + lane;
+            const int64_t left = end - cur;
+            const int rem = left < kStreamU * 32 ? (int)left : kStreamU * 32;
             int32_t j[kStreamU];
 #pragma unroll
-            for (int u = 0; u < kStreamU; ++u) {
-                const int64_t idx = cur + u * 32 + lane;
-                j[u] = idx < end ? __ldg(members + idx) : 0x7fffffff;
-            }
-            int taken = 0;
+            for (int u = 0; u < kStreamU; ++u)
+                j[u] = u * 32 + lane < rem ? __ldg(base + u * 32) : 0x7fffffff;
+            int mine = 0;
 #pragma unroll
             for (int u = 0; u < kStreamU; ++u) {
                 const bool ok = j[u] < jl;
                 if (ok) op(j[u], p);
-                taken += __popc(__ballot_sync(0xffffffffu, ok));
+                mine += ok;
             }
+            const int taken = __reduce_add_sync(0xffffffffu, mine);
             cur += taken;
             if (taken != kStreamU * 32) break;
         }
