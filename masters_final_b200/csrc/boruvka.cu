@@ -26,6 +26,7 @@
 #include "eacb_common.cuh"
 #include "scan_impl.cuh"
 
+#include <algorithm>
 #include <vector>
 
 namespace eacb {
@@ -433,7 +434,7 @@ k_whist_csr(const WT *weight, int64_t E, int wbits, unsigned long long *hist)
 // atomics): counts[warp][bin][lane], 32 KB per warp, two warps per block.
 constexpr int kHist8Threads = 64;
 constexpr size_t kHist8Smem = (size_t)(kHist8Threads / 32) * 256 * 32 * sizeof(uint32_t);
-__global__ void __launch_bounds__(kHist8Threads)
+__global__ void __launch_bounds__(kHist8Threads, 1)
 k_whist_u8(const uint8_t *w, int64_t n, unsigned long long *hist)
 {
     extern __shared__ uint32_t hs[];
@@ -445,12 +446,27 @@ k_whist_u8(const uint8_t *w, int64_t n, unsigned long long *hist)
     const int64_t nv = (n - head) >> 4;               // whole 16-byte vectors
     const uint4 *v = reinterpret_cast<const uint4 *>(w + head);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nv; q += stride) {
-        const uint4 x = __ldcs(v + q);
+    auto add16 = [&](const uint4 &x) {
         const uint32_t wd[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
         for (int k = 0; k < 16; ++k) mine[((wd[k >> 2] >> (8 * (k & 3))) & 255u) * 32] += 1;
+    };
+    // few warps fit beside the private columns, so each thread keeps eight
+    // 16-byte loads in flight
+    constexpr int kU = 8;
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; q + (kU - 1) * stride < nv; q += kU * stride) {
+        uint4 x[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) x[u] = __ldcs(v + q + u * stride);
+        // all eight loads are issued before the first is consumed
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+            asm volatile("" : "+r"(x[u].x), "+r"(x[u].y), "+r"(x[u].z), "+r"(x[u].w));
+#pragma unroll
+        for (int u = 0; u < kU; ++u) add16(x[u]);
     }
+    for (; q < nv; q += stride) add16(__ldcs(v + q));
     // the unaligned head and the ragged tail (< 32 bytes), by the first block
     if (blockIdx.x == 0) {
         const int64_t tail0 = head + (nv << 4);
@@ -689,81 +705,158 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
 
 // Same for an upper-triangle CSR with uint8 weights: both directions of each
 // kept entry.  Co-association rows are long (thousands of entries), so a
-// warp takes one row, counts its kept entries, and after the block's
-// reservation writes them in a second pass over the (now cached) row.
-__global__ void __launch_bounds__(kPhThreads)
+// warp takes one row and walks it in 128-entry groups, each lane taking four
+// consecutive entries: their four weights (one word) are read first, and the
+// four column indices (16 bytes) only when one of the weights falls in the
+// phase's range, so a phase over a narrow range reads little more than the
+// weight array; only those entries gather the other end's label.  A first
+// walk (four groups in flight) counts the kept entries, the warp reserves
+// 2 x that many words with one atomic, and a second walk over the (now
+// cached) row writes them: per group its i -> j words, then its j -> i words,
+// runs of equal source for the min-edge selection of later rounds.  Each
+// entry is checked (j > i, j < n) in the phase whose range holds its weight.
+__global__ void __launch_bounds__(kPhThreads, 4)
 k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, int32_t n,
-              int64_t nnz, int lo, int hi, int64_t row0, int64_t row1, const int32_t *label,
-              Pack pk, uint64_t *eout, unsigned long long *cursor, unsigned long long cap,
-              unsigned long long *best, int *err)
+              int64_t nnz, int lo, int hi, int dense, int64_t row0, int64_t row1,
+              const int32_t *label, Pack pk, uint64_t *eout, unsigned long long *cursor,
+              unsigned long long cap, unsigned long long *best, int *err)
 {
-    __shared__ int64_t s_cnt[kPhWarps];
-    __shared__ unsigned long long s_base;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
-    for (int64_t r0 = row0 + (int64_t)blockIdx.x * kPhWarps; r0 < row1;
-         r0 += (int64_t)gridDim.x * kPhWarps) {
-        const int64_t i = r0 + warp;
-        int64_t s = 0, e_end = 0;
-        int32_t li = 0;
-        if (i < row1) {
-            s = indptr[i];
-            e_end = indptr[i + 1];
-            if (s < 0 || e_end < s || e_end > nnz) {
-                if (lane == 0) set_err(err, DEV_BAD_INPUT);
-                e_end = s;
-            } else {
-                li = label[i];
-            }
+    constexpr int G = 4;
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = (int64_t)gridDim.x * kPhWarps;
+    for (int64_t i = row0 + (int64_t)blockIdx.x * kPhWarps + (threadIdx.x >> 5); i < row1;
+         i += nwarps) {
+        const int64_t s = indptr[i], e_end = indptr[i + 1];
+        if (s < 0 || e_end < s || e_end > nnz) {
+            if (lane == 0) set_err(err, DEV_BAD_INPUT);
+            continue;
         }
-        auto test = [&](int64_t e, uint32_t &ww, int32_t &j, int32_t &lj) -> bool {
-            if (e >= e_end) return false;
-            j = indices[e];
-            if (j <= i || j >= n) {
-                set_err(err, DEV_BAD_INPUT);
-                return false;
-            }
-            ww = w[e];
-            if ((int)ww <= lo || (int)ww > hi) return false;
-            lj = label[j];
-            return lj != li;
+        if (s == e_end) continue;
+        const int32_t li = label[i];
+        const int64_t a0 = s & ~(int64_t)3;        // groups start on 16-byte index boundaries
+        // weights of the lane's entries e .. e+3 (zero outside the arrays)
+        auto wload = [&](int64_t e) -> uint32_t {
+            if (e >= e_end) return 0u;
+            if (e + 3 < nnz) return __ldg(reinterpret_cast<const uint32_t *>(w + e));
+            uint32_t v = 0u;
+            for (int q = 0; q < 4 && e + q < nnz; ++q) v |= (uint32_t)w[e + q] << (8 * q);
+            return v;
         };
-        int64_t cnt = 0;
-        for (int64_t e0 = s; e0 < e_end; e0 += 32) {
-            uint32_t ww;
-            int32_t j, lj;
-            cnt += __popc(__ballot_sync(0xffffffffu, test(e0 + lane, ww, j, lj)));
-        }
-        if (lane == 0) s_cnt[warp] = cnt;
-        const bool fits = phase_reserve(s_cnt, &s_base, cursor, 2, cap, err);
-        if (cnt && fits) {
-            unsigned long long at = s_base + 2ull * (unsigned long long)s_cnt[warp];
-            uint64_t m = kNone;
-            for (int64_t e0 = s; e0 < e_end; e0 += 32) {
-                uint32_t ww = 0;
-                int32_t j = 0, lj = 0;
-                const bool keep = test(e0 + lane, ww, j, lj);
-                const unsigned bal = __ballot_sync(0xffffffffu, keep);
-                if (keep) {
-                    // the chunk's i -> j words, then its j -> i words: runs of
-                    // equal source for the min-edge selection of later rounds
-                    const uint64_t k = pk.make(ww, (uint32_t)i, (uint32_t)j);
-                    const unsigned long long p = at + __popc(bal & lt);
-                    eout[p] = k;
-                    eout[p + __popc(bal)] = k | 1ull;
-                    m = (k >> 1) < m ? (k >> 1) : m;
-                    min_if_lower(&best[lj], k >> 1);
+        // bit q: entry e+q is in the row with its weight in (lo, hi]
+        auto cmask = [&](int64_t e, uint32_t wv) -> unsigned {
+            unsigned m = 0u;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int ww = (int)((wv >> (8 * q)) & 255u);
+                m |= (e + q >= s && e + q < e_end && ww > lo && ww <= hi ? 1u : 0u) << q;
+            }
+            return m;
+        };
+        // the indices of the entries in cm (all four in a dense phase)
+        auto jload = [&](int64_t e, unsigned cm) -> int4 {
+            if (dense) cm = e < e_end ? 15u : 0u;
+            if (!cm) return make_int4(0, 0, 0, 0);
+            if (e + 3 < nnz) return __ldg(reinterpret_cast<const int4 *>(indices + e));
+            int32_t t[4] = {0, 0, 0, 0};
+            for (int q = 0; q < 4; ++q)
+                if (((cm >> q) & 1u) && e + q < nnz) t[q] = indices[e + q];
+            return make_int4(t[0], t[1], t[2], t[3]);
+        };
+        // bit q: candidate q is kept (other end in another component); lj
+        // receives the candidates' other-end labels
+        auto keep = [&](unsigned cm, const int4 &jv, int32_t (&lj)[4]) -> unsigned {
+            const int32_t jj[4] = {jv.x, jv.y, jv.z, jv.w};
+            unsigned c2 = cm;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (((cm >> q) & 1u) && (jj[q] <= i || jj[q] >= n)) {
+                    set_err(err, DEV_BAD_INPUT);
+                    c2 &= ~(1u << q);
                 }
-                at += 2ull * __popc(bal);
             }
 #pragma unroll
-            for (int o = 16; o >= 1; o >>= 1) {
-                const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
-                m = x < m ? x : m;
+            for (int q = 0; q < 4; ++q) lj[q] = ((c2 >> q) & 1u) ? label[jj[q]] : li;
+            unsigned km = 0u;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) km |= (lj[q] != li ? 1u : 0u) << q;
+            return km;
+        };
+        int cnt = 0;
+        for (int64_t g = a0; g < e_end; g += 128 * G) {
+            uint32_t wv[G];
+            unsigned cm[G];
+            int4 jv[G];
+            if (dense) {
+                // most entries are in range: the indices are read beside the
+                // weights instead of after them
+#pragma unroll
+                for (int u = 0; u < G; ++u) {
+                    wv[u] = wload(g + 128 * u + 4 * lane);
+                    jv[u] = jload(g + 128 * u + 4 * lane, 0u);
+                }
+#pragma unroll
+                for (int u = 0; u < G; ++u) cm[u] = cmask(g + 128 * u + 4 * lane, wv[u]);
+            } else {
+#pragma unroll
+                for (int u = 0; u < G; ++u) wv[u] = wload(g + 128 * u + 4 * lane);
+#pragma unroll
+                for (int u = 0; u < G; ++u) {
+                    cm[u] = cmask(g + 128 * u + 4 * lane, wv[u]);
+                    jv[u] = jload(g + 128 * u + 4 * lane, cm[u]);
+                }
             }
-            if (lane == 0 && m != kNone) min_if_lower(&best[li], m);
+#pragma unroll
+            for (int u = 0; u < G; ++u) {
+                int32_t lj[4];
+                cnt += __popc(keep(cm[u], jv[u], lj));
+            }
         }
-        __syncthreads();
+        cnt = __reduce_add_sync(0xffffffffu, cnt);
+        if (cnt == 0) continue;
+        unsigned long long at = 0;
+        if (lane == 0) at = atomicAdd(cursor, 2ull * (unsigned long long)cnt);
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (at + 2ull * (unsigned long long)cnt > cap) {
+            if (lane == 0) set_err(err, DEV_CAPACITY);
+            continue;
+        }
+        uint64_t m = kNone;
+        for (int64_t g = a0; g < e_end; g += 128) {
+            const int64_t e = g + 4 * lane;
+            const uint32_t wv = wload(e);
+            const unsigned cm = cmask(e, wv);
+            const int4 jv = jload(e, cm);
+            int32_t lj[4];
+            const unsigned km = keep(cm, jv, lj);
+            const int c = __popc(km);
+            int incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int o = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += o;
+            }
+            const int tot = __shfl_sync(0xffffffffu, incl, 31);
+            if (tot == 0) continue;
+            unsigned long long p = at + (unsigned long long)(incl - c);
+            const int32_t jj[4] = {jv.x, jv.y, jv.z, jv.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (!((km >> q) & 1u)) continue;
+                const uint64_t k = pk.make((wv >> (8 * q)) & 255u, (uint32_t)i, (uint32_t)jj[q]);
+                eout[p] = k;
+                eout[p + tot] = k | 1ull;
+                m = (k >> 1) < m ? (k >> 1) : m;
+                min_if_lower(&best[lj[q]], k >> 1);
+                ++p;
+            }
+            at += 2ull * (unsigned long long)tot;
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
+            m = x < m ? x : m;
+        }
+        if (lane == 0 && m != kNone) min_if_lower(&best[li], m);
     }
 }
 
@@ -1693,16 +1786,23 @@ static int64_t final_edge_cap(int32_t n, int64_t nnz)
     return want < all ? want : all;
 }
 
-// Phases of the final clustering: the weight ranges of the cumulative
-// fractions (0.125, 0.5, 1), each cut further so that its entries fit the
-// edge array (cap_entries upper entries, i.e. 2 cap_entries words); a single
-// weight with more entries than that is split by row ranges (the order
-// (w, a, b) keeps a row range of one weight contiguous).
+// Phases of the final clustering, lightest weights first: the weight ranges
+// whose cumulative entry counts reach ~8n, ~128n and all entries, each cut
+// further so that its entries fit the edge array (cap_entries upper entries,
+// i.e. 2 cap_entries words); a single weight with more entries than that is
+// split by row ranges (the order (w, a, b) keeps a row range of one weight
+// contiguous).  A co-association matrix holds thousands of entries per row,
+// and the lightest few per point already join most points: later phases
+// keep only entries between different components, so they write few edges
+// and their cost is the pass over the matrix.
 static int plan_final_phases(const unsigned long long h[256], int64_t cap_entries,
                              const int64_t *d_indptr, int32_t n, cudaStream_t st,
                              std::vector<Phase> &plan)
 {
-    const double fracs[3] = {0.125, 0.5, 1.0};
+    unsigned long long tot = 0;
+    for (int b = 0; b < 256; ++b) tot += h[b];
+    const double t = tot ? (double)tot : 1.0;
+    const double fracs[3] = {std::min(1.0, 8.0 * n / t), std::min(1.0, 128.0 * n / t), 1.0};
     int lo[8], hi[8];
     const int np = phase_ranges(h, fracs, 3, lo, hi);
     std::vector<int64_t> ip;     // host row pointers, fetched only if a weight needs splitting
@@ -1793,11 +1893,20 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
     if ((s = g.read_hist(st, wh))) return s;
     std::vector<Phase> phases;
     if ((s = plan_final_phases(wh, g.Emax / 2, indptr, n, st, phases))) return s;
+    unsigned long long wtot = 0;
+    for (int b = 0; b < 256; ++b) wtot += wh[b];
+    // a phase whose range holds over a quarter of the entries reads every
+    // 16-byte run of indices anyway
+    auto dense = [&](const Phase &ph) -> int {
+        unsigned long long in = 0;
+        for (int b = ph.lo + 1; b <= ph.hi; ++b) in += wh[b];
+        return 4 * in > wtot ? 1 : 0;
+    };
     auto build = [&](const Phase &ph) -> int {
         if (nnz == 0) return EACB_OK;
         ProfScope ps(PROF_PHASE, st);
         k_phase_upper<<<grid_for((ph.r1 - ph.r0) * 32, kPhThreads), kPhThreads, 0, st>>>(
-            indptr, indices, diassoc, n, nnz, ph.lo, ph.hi, ph.r0, ph.r1, g.label, pk, g.ea,
+            indptr, indices, diassoc, n, nnz, ph.lo, ph.hi, dense(ph), ph.r0, ph.r1, g.label, pk, g.ea,
             (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best, g.err);
         EACB_CHECK_LAUNCH();
         // compulsory reads: row pointers and labels (12 B per row), column and
