@@ -446,8 +446,43 @@ __global__ void k_label_exact_tc(const float *__restrict__ X, int32_t n, int32_t
     if (*err != 0) return;                      // k_exact_all did every point
     const int64_t cap = (int64_t)P * n;
     const int m = (int)min((int64_t)*namb, cap);
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
-        exact_label_point(X, n, D, C, kk, kmax, amb[t], labels, dists);
+    // one warp per point: lane l evaluates centroids l, l + 32, ... with the
+    // reference's arithmetic, and the warp keeps the smallest distance, the
+    // smallest index among equal ones (the reference loop's first minimum)
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < m; t += nw) {
+        const int64_t o = amb[t];
+        const int64_t p = o / n, i = o - p * n;
+        const int K = kk[p];
+        const float *x = X + i * D;
+        const float *Cp = C + p * kmax * D;
+        double best = 0.0;
+        int bl = 0x7fffffff;
+        for (int k = lane; k < K; k += 32) {
+            double dist = 0.0;
+            for (int d = 0; d < D; ++d) {
+                const float diff = __fsub_rn(x[d], Cp[(int64_t)k * D + d]);
+                dist = __dadd_rn(dist, (double)__fmul_rn(diff, diff));
+            }
+            if (k == lane || dist < best) {
+                best = dist;
+                bl = k;
+            }
+        }
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+            const int ok = __shfl_xor_sync(0xffffffffu, bl, off);
+            if (ok != 0x7fffffff && (bl == 0x7fffffff || ob < best || (!(best < ob) && ok < bl))) {
+                best = ob;
+                bl = ok;
+            }
+        }
+        if (lane == 0) {
+            labels[o] = bl;
+            dists[o] = (float)best;
+        }
     }
 }
 
@@ -522,7 +557,7 @@ int label_pass_tc(const float *X, int32_t n, int32_t D, int32_t P, const float *
     ps.done(0.0);
     k_exact_all<<<296, 256, 0, st>>>(X, n, D, C, kk, kmax, P, active, s.err, labels, dists);
     EACB_CHECK_LAUNCH();
-    k_label_exact_tc<<<148 * 4, 128, 0, st>>>(X, n, D, C, kk, kmax, P, amb, namb, s.err, labels,
+    k_label_exact_tc<<<148 * 8, 256, 0, st>>>(X, n, D, C, kk, kmax, P, amb, namb, s.err, labels,
                                               dists);
     EACB_CHECK_LAUNCH();
     return EACB_OK;
