@@ -449,7 +449,8 @@ k_whist_u8(const uint8_t *w, int64_t n, unsigned long long *hist)
     auto add16 = [&](const uint4 &x) {
         const uint32_t wd[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-        for (int k = 0; k < 16; ++k) mine[((wd[k >> 2] >> (8 * (k & 3))) & 255u) * 32] += 1;
+        for (int k = 0; k < 16; ++k)     // no-return adds: equal bytes do not serialise
+            atomicAdd(&mine[((wd[k >> 2] >> (8 * (k & 3))) & 255u) * 32], 1u);
     };
     // few warps fit beside the private columns, so each thread keeps eight
     // 16-byte loads in flight
@@ -719,9 +720,13 @@ __global__ void __launch_bounds__(kPhThreads, 4)
 k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, int32_t n,
               int64_t nnz, int lo, int hi, int dense, int64_t row0, int64_t row1,
               const int32_t *label, Pack pk, uint64_t *eout, unsigned long long *cursor,
-              unsigned long long cap, unsigned long long *best, int *err)
+              unsigned long long cap, unsigned long long *best, unsigned long long *khist,
+              int *err)
 {
     constexpr int G = 4;
+    __shared__ unsigned s_kh[256];           // kept entries per weight, this block
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) s_kh[b] = 0u;
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int64_t nwarps = (int64_t)gridDim.x * kPhWarps;
     for (int64_t i = row0 + (int64_t)blockIdx.x * kPhWarps + (threadIdx.x >> 5); i < row1;
@@ -742,15 +747,20 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
             for (int q = 0; q < 4 && e + q < nnz; ++q) v |= (uint32_t)w[e + q] << (8 * q);
             return v;
         };
-        // bit q: entry e+q is in the row with its weight in (lo, hi]
+        // bit q: entry e+q is in the row with its weight in (lo, hi]; four
+        // byte compares at once, the row's bounds only in its edge groups
+        const uint32_t lo4 = 0x01010101u * (uint32_t)(lo + 1), hi4 = 0x01010101u * (uint32_t)hi;
         auto cmask = [&](int64_t e, uint32_t wv) -> unsigned {
-            unsigned m = 0u;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int ww = (int)((wv >> (8 * q)) & 255u);
-                m |= (e + q >= s && e + q < e_end && ww > lo && ww <= hi ? 1u : 0u) << q;
+            uint32_t m = __vcmpgeu4(wv, lo4) & __vcmpleu4(wv, hi4);
+            if (e < s || e + 4 > e_end) {
+                const int64_t a = s - e, b = e_end - e;     // valid bytes [a, b)
+                const int qa = a < 0 ? 0 : (a > 4 ? 4 : (int)a);
+                const int qb = b < 0 ? 0 : (b > 4 ? 4 : (int)b);
+                const uint32_t va = qa >= 4 ? 0u : 0xffffffffu << (8 * qa);
+                const uint32_t vb = qb <= 0 ? 0u : 0xffffffffu >> (8 * (4 - qb));
+                m &= va & vb;
             }
-            return m;
+            return ((m >> 7) & 1u) | ((m >> 14) & 2u) | ((m >> 21) & 4u) | ((m >> 28) & 8u);
         };
         // the indices of the entries in cm (all four in a dense phase)
         auto jload = [&](int64_t e, unsigned cm) -> int4 {
@@ -808,7 +818,10 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
 #pragma unroll
             for (int u = 0; u < G; ++u) {
                 int32_t lj[4];
-                cnt += __popc(keep(cm[u], jv[u], lj));
+                const unsigned km = keep(cm[u], jv[u], lj);
+                cnt += __popc(km);
+                for (unsigned b = km; b; b &= b - 1u)
+                    atomicAdd(&s_kh[(wv[u] >> (8 * (__ffs(b) - 1))) & 255u], 1u);
             }
         }
         cnt = __reduce_add_sync(0xffffffffu, cnt);
@@ -858,6 +871,9 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
         }
         if (lane == 0 && m != kNone) min_if_lower(&best[li], m);
     }
+    __syncthreads();
+    for (int b = threadIdx.x; b < 256; b += blockDim.x)
+        if (s_kh[b]) atomicAdd(&khist[b], (unsigned long long)s_kh[b]);
 }
 
 // One phase: the entries with weight bucket in (lo, hi] of rows [r0, r1);
@@ -1203,6 +1219,7 @@ struct Engine {
         for (const Phase &ph : plan) {
             EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V, st));
             EACB_CUDA(cudaMemsetAsync(&cnt[C_CURSOR], 0, sizeof(int64_t), st));
+            EACB_CUDA(cudaMemsetAsync(hist, 0, 256 * sizeof(unsigned long long), st));
             int s = build(ph);
             if (s) return s;
             int64_t Ep = 0;
@@ -1218,6 +1235,58 @@ struct Engine {
             if ((s = run<SEL_MST>(pk, Ep, V, st, &nm, &nc))) return s;
             mst_base += nm;
             V = (int32_t)nc;
+            if (V <= 1) break;
+        }
+        *n_mst_out = mst_base;
+        *n_comp_out = V;
+        return EACB_OK;
+    }
+
+    // Phases in order with a host read after each build (the final
+    // clustering): the edge array holds a phase's usual output, and a phase
+    // whose kept entries overflow it is discarded and redone as the pieces
+    // split() cuts from the build's per-weight kept counts, in order.
+    template <typename Build, typename Split>
+    int run_phased_retry(Pack pk, std::vector<Phase> plan, Build build, Split split,
+                         cudaStream_t st, int64_t *n_mst_out, int64_t *n_comp_out)
+    {
+        int32_t V = V0;
+        mst_base = 0;
+        size_t q = 0;
+        while (q < plan.size()) {
+            const Phase ph = plan[q];
+            EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V, st));
+            EACB_CUDA(cudaMemsetAsync(&cnt[C_CURSOR], 0, sizeof(int64_t), st));
+            EACB_CUDA(cudaMemsetAsync(hist, 0, 256 * sizeof(unsigned long long), st));
+            int s = build(ph);
+            if (s) return s;
+            int64_t Ep = 0;
+            int e = 0;
+            EACB_CUDA(cudaMemcpyAsync(&Ep, &cnt[C_CURSOR], sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                      st));
+            EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+            EACB_CUDA(cudaStreamSynchronize(st));
+            if (e == DEV_CAPACITY) {
+                // the build still counted every kept entry, per weight, in
+                // hist: the pieces are cut from those counts
+                unsigned long long kh[256];
+                EACB_CUDA(cudaMemcpyAsync(kh, hist, sizeof(kh), cudaMemcpyDeviceToHost, st));
+                EACB_CUDA(cudaStreamSynchronize(st));
+                std::vector<Phase> pieces;
+                if ((s = split(ph, kh, pieces))) return s;
+                EACB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+                plan.erase(plan.begin() + (ptrdiff_t)q);
+                plan.insert(plan.begin() + (ptrdiff_t)q, pieces.begin(), pieces.end());
+                continue;
+            }
+            if (e) return dev_err_to_status(e);
+            if (Ep > Emax) return EACB_ERR_INTERNAL;
+            if (prof().enabled) prof().bytes[PROF_PHASE] += 8.0 * (double)Ep;   // words written
+            int64_t nm = 0, nc = 0;
+            if ((s = run<SEL_MST>(pk, Ep, V, st, &nm, &nc))) return s;
+            mst_base += nm;
+            V = (int32_t)nc;
+            ++q;
             if (V <= 1) break;
         }
         *n_mst_out = mst_base;
@@ -1778,66 +1847,96 @@ extern "C" int eacb_connected_components(const int32_t *dest, const void *weight
 // never holds more than half the entries (both directions: nnz words), and
 // at least 8 n + 2^20 words (every row fits, and the forest's 2 (n - 1)),
 // so the workspace stays near 8 bytes per entry instead of 16.
+// Edge words of the final clustering: every entry's two directions when the
+// matrix is small, else 256 words per point (at least 2^20): room for the
+// usual output of a phase, not its worst case (a phase that overflows is
+// redone in halves), so a matrix of thousands of entries per row does not
+// need an edge array of its own size.
 static int64_t final_edge_cap(int32_t n, int64_t nnz)
 {
-    const int64_t lo = 8 * (int64_t)n + (1 << 20);
-    const int64_t want = nnz > lo ? nnz : lo;
-    const int64_t all = 2 * nnz > 2 * (int64_t)n ? 2 * nnz : 2 * (int64_t)n;
-    return want < all ? want : all;
+    const int64_t all = 2 * (nnz > (int64_t)n ? nnz : (int64_t)n);
+    const int64_t usual = 256 * (int64_t)n > ((int64_t)1 << 20) ? 256 * (int64_t)n : ((int64_t)1 << 20);
+    return all < usual ? all : usual;
 }
 
 // Phases of the final clustering, lightest weights first: the weight ranges
-// whose cumulative entry counts reach ~8n, ~128n and all entries, each cut
-// further so that its entries fit the edge array (cap_entries upper entries,
-// i.e. 2 cap_entries words); a single weight with more entries than that is
-// split by row ranges (the order (w, a, b) keeps a row range of one weight
-// contiguous).  A co-association matrix holds thousands of entries per row,
-// and the lightest few per point already join most points: later phases
-// keep only entries between different components, so they write few edges
-// and their cost is the pass over the matrix.
-static int plan_final_phases(const unsigned long long h[256], int64_t cap_entries,
-                             const int64_t *d_indptr, int32_t n, cudaStream_t st,
-                             std::vector<Phase> &plan)
+// whose cumulative entry counts reach 8n, 32n, 128n, 512n, 2048n and all
+// entries.  A co-association matrix holds thousands of entries per row, and
+// the lightest few per point already join most points: later phases keep
+// only entries between different components, so they write few edges, and a
+// phase over a narrow range reads little more than the weights.
+static void plan_final_phases(const unsigned long long h[256], int32_t n, std::vector<Phase> &plan)
 {
     unsigned long long tot = 0;
     for (int b = 0; b < 256; ++b) tot += h[b];
     const double t = tot ? (double)tot : 1.0;
-    const double fracs[3] = {std::min(1.0, 8.0 * n / t), std::min(1.0, 128.0 * n / t), 1.0};
+    double fracs[6];
+    for (int f = 0; f < 5; ++f) fracs[f] = std::min(1.0, (double)(8 << (2 * f)) * n / t);
+    fracs[5] = 1.0;
     int lo[8], hi[8];
-    const int np = phase_ranges(h, fracs, 3, lo, hi);
-    std::vector<int64_t> ip;     // host row pointers, fetched only if a weight needs splitting
-    for (int q = 0; q < np; ++q) {
-        int start = lo[q];        // current range is (start, b]
-        unsigned long long acc = 0;
-        for (int b = lo[q] + 1; b <= hi[q]; ++b) {
-            if (acc + h[b] <= (unsigned long long)cap_entries) {
-                acc += h[b];
-                continue;
-            }
-            if (acc) plan.push_back(Phase{start, b - 1, 0, n, -1});
-            start = b - 1;
-            acc = 0;
-            if (h[b] <= (unsigned long long)cap_entries) {
-                acc = h[b];
-                continue;
-            }
-            // weight b alone: rows in pieces of at most cap_entries entries
-            if (ip.empty()) {
-                ip.resize((size_t)n + 1);
-                EACB_CUDA(cudaMemcpyAsync(ip.data(), d_indptr, sizeof(int64_t) * ((size_t)n + 1),
-                                          cudaMemcpyDeviceToHost, st));
-                EACB_CUDA(cudaStreamSynchronize(st));
-            }
-            int64_t r0 = 0;
-            while (r0 < n) {
-                int64_t r1 = r0 + 1;
-                while (r1 < n && ip[r1 + 1] - ip[r0] <= cap_entries) ++r1;
-                plan.push_back(Phase{b - 1, b, r0, r1, -1});
-                r0 = r1;
-            }
-            start = b;
+    const int np = phase_ranges(h, fracs, 6, lo, hi);
+    for (int q = 0; q < np; ++q) plan.push_back(Phase{lo[q], hi[q], 0, n, -1});
+}
+
+// Pieces of a phase whose kept entries did not fit the edge array, from the
+// kept entries per weight that its build counted (kh; upper bounds for the
+// pieces, whose components only merge): consecutive weights while their
+// kept entries fit, and a weight that alone does not fit split into row
+// ranges of equal entry counts (the order (w, a, b) keeps a row range of one
+// weight contiguous).  Host row pointers are fetched on the first row split.
+static int split_final_phase(const Phase &ph, const unsigned long long kh[256], int64_t cap_entries,
+                             const int64_t *d_indptr, int32_t n, std::vector<int64_t> &ip,
+                             cudaStream_t st, std::vector<Phase> &out)
+{
+    const unsigned long long cap = (unsigned long long)(cap_entries / 8 * 7);
+    if (ph.r0 != 0 || ph.r1 != n) {
+        // a row range of one weight: halve the rows
+        if (ph.r1 - ph.r0 < 2) return EACB_ERR_INTERNAL;
+        const int64_t m = ph.r0 + (ph.r1 - ph.r0) / 2;
+        out.push_back(Phase{ph.lo, ph.hi, ph.r0, m, -1});
+        out.push_back(Phase{ph.lo, ph.hi, m, ph.r1, -1});
+        return EACB_OK;
+    }
+    int start = ph.lo;
+    unsigned long long acc = 0;
+    for (int w = ph.lo + 1; w <= ph.hi; ++w) {
+        if (kh[w] <= cap && acc + kh[w] <= cap) {
+            acc += kh[w];
+            continue;
         }
-        if (acc) plan.push_back(Phase{start, hi[q], 0, n, -1});
+        if (w - 1 > start) out.push_back(Phase{start, w - 1, 0, n, -1});
+        if (kh[w] <= cap) {                    // w opens the next piece
+            start = w - 1;
+            acc = kh[w];
+            continue;
+        }
+        // weight w alone: rows in pieces of about equal entry counts
+        if (ip.empty()) {
+            ip.resize((size_t)n + 1);
+            EACB_CUDA(cudaMemcpyAsync(ip.data(), d_indptr, sizeof(int64_t) * ((size_t)n + 1),
+                                      cudaMemcpyDeviceToHost, st));
+            EACB_CUDA(cudaStreamSynchronize(st));
+        }
+        const int64_t parts = (int64_t)((kh[w] + cap - 1) / cap);
+        const double piece = (double)ip[n] / (double)parts;
+        int64_t r = 0;
+        while (r < n) {
+            int64_t e = r + 1;
+            while (e < n && (double)(ip[e + 1] - ip[r]) <= piece) ++e;
+            out.push_back(Phase{w - 1, w, r, e, -1});
+            r = e;
+        }
+        start = w;
+        acc = 0;
+    }
+    if (ph.hi > start) out.push_back(Phase{start, ph.hi, 0, n, -1});
+    if (out.size() == 1 && out[0].lo == ph.lo && out[0].hi == ph.hi) {
+        // the counts say it fits (it cannot have overflowed): split anyway
+        out.clear();
+        if (ph.hi - ph.lo < 2) return EACB_ERR_INTERNAL;
+        const int m = ph.lo + (ph.hi - ph.lo) / 2;
+        out.push_back(Phase{ph.lo, m, 0, n, -1});
+        out.push_back(Phase{m, ph.hi, 0, n, -1});
     }
     return EACB_OK;
 }
@@ -1892,7 +1991,7 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
     unsigned long long wh[256];
     if ((s = g.read_hist(st, wh))) return s;
     std::vector<Phase> phases;
-    if ((s = plan_final_phases(wh, g.Emax / 2, indptr, n, st, phases))) return s;
+    plan_final_phases(wh, n, phases);
     unsigned long long wtot = 0;
     for (int b = 0; b < 256; ++b) wtot += wh[b];
     // a phase whose range holds over a quarter of the entries reads every
@@ -1907,7 +2006,8 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
         ProfScope ps(PROF_PHASE, st);
         k_phase_upper<<<grid_for((ph.r1 - ph.r0) * 32, kPhThreads), kPhThreads, 0, st>>>(
             indptr, indices, diassoc, n, nnz, ph.lo, ph.hi, dense(ph), ph.r0, ph.r1, g.label, pk, g.ea,
-            (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best, g.err);
+            (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best, g.hist,
+            g.err);
         EACB_CHECK_LAUNCH();
         // compulsory reads: row pointers and labels (12 B per row), column and
         // weight (5 B per entry; a row-range phase is counted in proportion to
@@ -1916,7 +2016,11 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
         ps.done(12.0 * rows + 5.0 * (double)nnz * (rows / (double)n));
         return EACB_OK;
     };
-    if ((s = g.run_phased(pk, phases, build, st, &n_mst, &n_comp))) return s;
+    std::vector<int64_t> hip;
+    auto split = [&](const Phase &ph, const unsigned long long kh[256], std::vector<Phase> &out) {
+        return split_final_phase(ph, kh, g.Emax / 2, indptr, n, hip, st, out);
+    };
+    if ((s = g.run_phased_retry(pk, phases, build, split, st, &n_mst, &n_comp))) return s;
     // 2. lifetime rule on the weight histogram
     EACB_CUDA(cudaMemsetAsync(hist, 0, 256 * sizeof(int64_t), st));
     if (n_mst > 0) {

@@ -195,8 +195,8 @@ def test_final_clustering_disconnected(T):
 
 def test_final_clustering_capacity_split_phases(T):
     """More entries than the final clustering's edge array holds at once, with
-    one weight owning most of them: the weight is processed in row-range
-    phases (the forest and the labels must not change)."""
+    one weight owning most of them: the workspace stays below the matrix's
+    own size and the forest and the labels do not change."""
     from masters_final_b200 import _lib
     from masters_final_b200.EAC.eac import sp_sl_lifetime_csr
     rng = np.random.default_rng(8)
@@ -215,6 +215,35 @@ def test_final_clustering_capacity_split_phases(T):
     for P in (59, 80):
         nc, labels = sp_sl_lifetime_csr(indptr, b.astype(np.int32), w, n, P)
         nc2, lab2 = oracle.sp_sl_lifetime(n, a, b, w, P)
+        assert nc == nc2
+        if nc > 1:
+            assert np.array_equal(labels, lab2)
+
+
+def test_final_clustering_overflow_retry(T):
+    """A complete graph whose lightest weights hold more entries than the edge
+    array: the first phase overflows, is redone as weight pieces, and the
+    piece of weight 2 overflows again and is redone as row ranges.  Forest
+    and labels must equal the oracle's."""
+    from masters_final_b200 import _lib
+    from masters_final_b200.EAC.eac import sp_sl_lifetime_csr
+    rng = np.random.default_rng(12)
+    n = 2000
+    a, b = np.triu_indices(n, 1)
+    m = a.size                                      # 1,999,000 entries
+    group = rng.integers(0, 3, n)                   # three groups joined by heavy entries
+    inside = group[a] == group[b]
+    w = np.where(inside, rng.integers(3, 60, m), rng.integers(150, 200, m)).astype(np.uint8)
+    pick = rng.permutation(np.nonzero(inside)[0])
+    w[pick[:10_000]] = 1
+    w[pick[10_000:610_000]] = 2                     # 600k entries: 1.2M words > 2^20
+    L = _lib.load()
+    assert L.eacb_final_clustering_workspace_size(n, m) < 8 * 2 * m
+    indptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(a, minlength=n), out=indptr[1:])
+    for P in (199, 250):
+        nc, labels = sp_sl_lifetime_csr(indptr, b.astype(np.int32), w, n, P)
+        nc2, lab2 = oracle.sp_sl_lifetime(n, a.astype(np.int64), b.astype(np.int64), w, P)
         assert nc == nc2
         if nc > 1:
             assert np.array_equal(labels, lab2)
