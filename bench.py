@@ -72,14 +72,36 @@ class ClockSampler:
             self.f = open(self.out, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index),
                                           "--query-gpu=" + q, "--format=csv,noheader,nounits",
-                                          "-lms", "100"], stdout=self.f,
+                                          "-lms", "50"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+        # the timed region is short (milliseconds): it starts only once the
+        # sampler has written its first line
+        self.lines0 = self._wait_lines(1, 5.0)
         return self
+
+    def _lines(self):
+        try:
+            with open(self.out) as f:
+                return sum(1 for _ in f)
+        except OSError:
+            return 0
+
+    def _wait_lines(self, at_least, timeout_s):
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < timeout_s:
+            self.f.flush()
+            k = self._lines()
+            if k >= at_least:
+                return k
+            time.sleep(0.005)
+        return self._lines()
 
     def __exit__(self, *a):
         if self.proc is not None:
+            # one more sample after the region, so that it is bracketed
+            self._wait_lines(self.lines0 + 1, 2.0)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
