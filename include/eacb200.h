@@ -11,7 +11,8 @@
  *   - `stream` is a cudaStream_t cast to uintptr_t (0 = legacy default stream);
  *   - scratch memory is a caller-owned device buffer `ws` of `ws_bytes` bytes,
  *     at least the size returned by the matching *_workspace_size() query,
- *     256-byte aligned; the library never allocates device memory;
+ *     256-byte aligned (a misaligned one gives EACB_ERR_WORKSPACE); the
+ *     library never allocates device memory;
  *   - functions return an eacb_status (0 = success, negative = error) and
  *     never throw; outputs are undefined after an error;
  *   - functions whose work has data-dependent sizes (Boruvka, connected
@@ -35,7 +36,7 @@ extern "C" {
 typedef enum {
     EACB_OK = 0,
     EACB_ERR_BAD_ARGUMENT = -1,          /* null pointer, negative size, bad enum */
-    EACB_ERR_WORKSPACE = -2,             /* ws too small or an internal capacity exceeded */
+    EACB_ERR_WORKSPACE = -2,             /* ws too small or misaligned, or an internal capacity exceeded */
     EACB_ERR_CUDA = -3,                  /* a CUDA runtime call failed */
     EACB_ERR_UNSUPPORTED = -4,           /* valid input this build does not handle */
     EACB_ERR_DEVICE_WAIT = -5,           /* a bounded device-side wait gave up */

@@ -17,6 +17,7 @@ _DTYPE_CODE = {np.dtype(np.uint8): U8, np.dtype(np.uint16): U16, np.dtype(np.int
 
 ERR_VALUE = -9
 ERR_FIRST_OVERFLOW = -7
+ERR_WORKSPACE = -2
 
 _lib = None
 

@@ -77,7 +77,12 @@ struct Carver {
     size_t off;
     size_t cap;
     bool overflow;
-    explicit Carver(void *b, size_t c) : base((char *)b), off(0), cap(c), overflow(false) {}
+    // a workspace that is not 256-byte aligned is refused like a short one
+    // (the tensor-core and vector paths need 16-byte aligned sub-buffers)
+    explicit Carver(void *b, size_t c)
+        : base((char *)b), off(0), cap(c), overflow(b != nullptr && ((uintptr_t)b & 255u) != 0)
+    {
+    }
     template <typename T>
     T *take(size_t count)
     {

@@ -345,12 +345,21 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
         const float *ncp = nc + ((int64_t)p * kt_max + t) * kTN;
         const int c_lo = colh, c_hi = min(colh + 128, nvalid);
         for (int c0 = c_lo; c0 < c_hi; c0 += 16) {
-            float v[16];
+            float v[16], ncv[16];
             tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c0, v);
+            // the 16 centroid norms, the same for every lane: four 16-byte loads
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float4 f = __ldg(reinterpret_cast<const float4 *>(ncp + c0) + q);
+                ncv[4 * q] = f.x;
+                ncv[4 * q + 1] = f.y;
+                ncv[4 * q + 2] = f.z;
+                ncv[4 * q + 3] = f.w;
+            }
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
                 const int c = c0 + j;
-                const float s = fmaf(-2.f, v[j], xn + __ldg(&ncp[c]));   // ncp[c] = +inf past K
+                const float s = fmaf(-2.f, v[j], xn + ncv[j]);   // ncp[c] = +inf past K
                 const bool lt = s < b1;
                 b2 = lt ? b1 : fminf(b2, s);
                 i1 = lt ? t * kTN + c : i1;

@@ -163,3 +163,23 @@ def test_python_step_wrappers(T):
         lifetime_cut_gpu(np.array([1], dtype=np.uint8), 10, 5)
     out, ng = relabel_canonical(g["final_labels"][::-1].copy())
     assert np.array_equal(out.cpu().numpy(), oracle.canonical_labels(g["final_labels"][::-1]))
+
+
+def test_misaligned_workspace_refused(T):
+    """A workspace that is not 256-byte aligned is refused before any launch."""
+    from masters_final_b200 import _lib
+    L = _lib.load()
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal((1000, 4)).astype(np.float32)
+    xd = T.from_numpy(x).cuda()
+    cd = xd[:10].clone()
+    lab = T.empty(1000, dtype=T.int32, device="cuda")
+    dist = T.empty(1000, dtype=T.float32, device="cuda")
+    nb = L.eacb_kmeans_label_workspace_size(1000, 4, 10)
+    ws = _ws(T, nb + 512)
+    st = L.eacb_kmeans_label_fp32(_lib.ptr(xd), 1000, 4, _lib.ptr(cd), 10, _lib.ptr(lab),
+                                  _lib.ptr(dist), ctypes.c_void_p(ws.data_ptr() + 16),
+                                  ws.numel() - 16, None)
+    assert st == _lib.ERR_WORKSPACE
+    _lib.check(L.eacb_kmeans_label_fp32(_lib.ptr(xd), 1000, 4, _lib.ptr(cd), 10, _lib.ptr(lab),
+                                        _lib.ptr(dist), _lib.ptr(ws), ws.numel(), None), "label")
