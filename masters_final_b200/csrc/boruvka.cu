@@ -1843,10 +1843,6 @@ extern "C" int eacb_connected_components(const int32_t *dest, const void *weight
                         n_edges, nullptr, &dummy, labels, host_n_comps, ws, ws_bytes, stream);
 }
 
-// Edge-array capacity of the final clustering (directed words).  A phase
-// never holds more than half the entries (both directions: nnz words), and
-// at least 8 n + 2^20 words (every row fits, and the forest's 2 (n - 1)),
-// so the workspace stays near 8 bytes per entry instead of 16.
 // Edge words of the final clustering: every entry's two directions when the
 // matrix is small, else 256 words per point (at least 2^20): room for the
 // usual output of a phase, not its worst case (a phase that overflows is

@@ -201,7 +201,7 @@ def test_final_clustering_capacity_split_phases(T):
     from masters_final_b200.EAC.eac import sp_sl_lifetime_csr
     rng = np.random.default_rng(8)
     n = 12_000
-    m = 2_600_000                                   # > 8 n + 2^20 upper entries
+    m = 2_600_000                                   # 2 m words > the edge array (256 n)
     a = rng.integers(0, n - 1, m)
     b = a + 1 + (rng.random(m) * (n - 1 - a)).astype(np.int64)
     key = np.unique(a * n + b)
