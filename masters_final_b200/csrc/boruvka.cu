@@ -1846,7 +1846,7 @@ extern "C" int eacb_connected_components(const int32_t *dest, const void *weight
 // Edge words of the final clustering: every entry's two directions when the
 // matrix is small, else 256 words per point (at least 2^20): room for the
 // usual output of a phase, not its worst case (a phase that overflows is
-// redone in halves), so a matrix of thousands of entries per row does not
+// redone in pieces), so a matrix of thousands of entries per row does not
 // need an edge array of its own size.
 static int64_t final_edge_cap(int32_t n, int64_t nnz)
 {
