@@ -20,6 +20,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -61,7 +62,9 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.out = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % index)
+        # raw samples (the summary goes into the JSON line)
+        self.out = os.path.join(os.environ.get("EACB_CLOCKS_DIR", tempfile.gettempdir()),
+                                "clocks_bench_%d.csv" % index)
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.out), exist_ok=True)
