@@ -40,14 +40,14 @@ namespace eacb {
 constexpr int kMaxK = 8192;            // largest cluster id + 1 supported
 constexpr int kRowThreads = 512;
 constexpr int kBitmapBytes = 96 * 1024;        // pass 1: 786,432 columns per chunk
-// pass 2 runs one 1024-thread CTA per SM with 192 KB of byte counters and a
-// "touched" flag byte per 16 counters: rows of large n span many column
-// chunks, and each chunk costs a walk step per tail; the compaction reads
-// only flagged counter vectors and clears what it reads, so a chunk costs no
-// pass over its mostly-zero counters
-constexpr int kFillThreads = 1024;
+// pass 2 runs two 512-thread CTAs per SM, each with 96 KB of byte counters
+// and a "touched" flag byte per 16 counters; the compaction reads only
+// flagged counter vectors and clears what it reads, so a chunk costs no pass
+// over its mostly-zero counters, and one CTA's compaction and barrier waits
+// overlap the other's walk
+constexpr int kFillThreads = 512;
 constexpr int kFillVecs = 12;                  // counter vectors (16 columns) per thread
-constexpr int kCountBytes = kFillThreads * kFillVecs * 16;   // 196,608 columns per chunk
+constexpr int kCountBytes = kFillThreads * kFillVecs * 16;   // 98,304 columns per chunk
 constexpr int kFillSmem = kCountBytes + kCountBytes / 16;
 constexpr int kCapCols = 16 * 1024;            // capped rows: columns per chunk
 constexpr int kCapSmem = kCapCols * 5;         // byte counters + 32-bit ranks
@@ -281,7 +281,7 @@ __device__ __forceinline__ int64_t emit_flagged(uint32_t *ctr32, uint32_t *flag3
     return tot;
 }
 
-__global__ void __launch_bounds__(kFillThreads, 1)
+__global__ void __launch_bounds__(kFillThreads, 2)
 k_rows_fill(TailCtx tc, const int32_t *rowperm, const int32_t *rowflag, const int64_t *indptr,
             int32_t *indices, uint8_t *data, int *queue, int *gmax, int *err)
 {
@@ -683,7 +683,7 @@ extern "C" int eacb_coassoc_fill(const int32_t *labels, int32_t n, int32_t P, in
     EACB_CUDA(allow_max_dyn_smem(k_rows_fill));
     EACB_CUDA(allow_max_dyn_smem(k_rows_capped));
     ProfScope ps(PROF_COASSOC, st);
-    k_rows_fill<<<row_grid(1), kFillThreads, kFillSmem, st>>>(
+    k_rows_fill<<<row_grid(2), kFillThreads, kFillSmem, st>>>(
         tc, w.rowperm, w.rowflag, indptr, indices, data, &w.queue[1], w.maxcnt, w.err);
     EACB_CHECK_LAUNCH();
     ps.done(0.0);
