@@ -330,48 +330,6 @@ __global__ void k_edges_csr(const int32_t *first, const int32_t *deg, const int3
     }
 }
 
-// Both directions of every entry of an upper-triangle CSR with uint8 weights.
-// Forward copies land at [e], reverse copies at [nnz + e].
-template <int MODE>
-__global__ void k_edges_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w,
-                              int32_t n, int64_t nnz, Pack pk, uint64_t *eout,
-                              unsigned long long *best, int *err)
-{
-    const int lane = threadIdx.x & 31;
-    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
-         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int64_t s = indptr[i], e_end = indptr[i + 1];
-        if (s < 0 || e_end < s || e_end > nnz) {
-            if (lane == 0) set_err(err, DEV_BAD_INPUT);
-            continue;
-        }
-        uint64_t m = kNone;
-        for (int64_t e = s + lane; e < e_end; e += 32) {
-            int32_t j = indices[e];
-            if (j <= i || j >= n) {
-                set_err(err, DEV_BAD_INPUT);
-                eout[e] = kNone;       // never selected: dropped by the first contraction
-                eout[nnz + e] = kNone;
-                continue;
-            }
-            uint32_t ww = w[e];
-            uint64_t f = pk.make(ww, (uint32_t)i, (uint32_t)j);
-            eout[e] = f;
-            eout[nnz + e] = f | 1ull;
-            uint64_t sel_f = MODE == SEL_MST ? (f >> 1) : (((uint64_t)ww << 32) | (uint32_t)j);
-            uint64_t sel_r = MODE == SEL_MST ? (f >> 1) : (((uint64_t)ww << 32) | (uint32_t)i);
-            m = sel_f < m ? sel_f : m;
-            atomicMin(&best[j], (unsigned long long)sel_r);
-        }
-#pragma unroll
-        for (int d = 16; d >= 1; d >>= 1) {
-            uint64_t o = __shfl_xor_sync(0xffffffffu, m, d);
-            m = o < m ? o : m;
-        }
-        if (lane == 0 && m != kNone) atomicMin(&best[i], (unsigned long long)m);
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Weight phases (MST mode).  For a strict total order of the edges, the
 // minimum spanning forest of the edges up to a key is exactly the MST
