@@ -185,31 +185,54 @@ def cpu_baseline(indptr, dest, w, n_edges, budget_s=12.0):
                       "boruvka_minho_seq (single-threaded, like the reference), median" % len(times)}
 
 
+def reference_threads():
+    """Host threads for the reference arm: every core this process may use,
+    bounded so that the concurrent copies (~0.4 GB each) fit in half of the
+    available memory."""
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    try:
+        import psutil
+        mem_cap = int(psutil.virtual_memory().available * 0.5 // (400 << 20))
+    except ImportError:
+        mem_cap = cores
+    return max(1, min(cores or 1, mem_cap, 64))
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    from concurrent.futures import ThreadPoolExecutor
     from masters_final_b200 import workloads as W
     indptr, dest, w = W.knn_graph(N_VERTICES, k=KNN, seed=SEED)
     n_edges = dest.size // 2
     import oracle
+    run = oracle.boruvka_seq_runner(indptr, dest, w)
+    # the reference's Boruvka is sequential: one graph cannot use more than
+    # one core, so every host thread runs its own copy of the graph and the
+    # throughput is all copies' edges over the wall time of a step
+    threads = reference_threads()
     times = []
-    for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        oracle.boruvka_seq(indptr, dest, w)
-        dt = time.perf_counter() - t0
-        if i >= args.warmup:
-            times.append(dt)
+    with ThreadPoolExecutor(threads) as ex:
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            done = list(ex.map(lambda _: run(), range(threads)))
+            dt = time.perf_counter() - t0
+            assert all(x == done[0] for x in done)
+            if i >= args.warmup:
+                times.append(dt)
     tot = sum(times)
-    val = n_edges * len(times) / tot
+    val = threads * n_edges * len(times) / tot
     line = {"metric": "MST edges/s", "value": val, "unit": "edges/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000 * tot / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
             "config": workload_config(n_edges),
-            "cpu_baseline": {"value": val, "unit": "edges/s", "cores": 1, "kind": "port",
-                             "sample": "full graph per step; the oracle's C restatement of "
-                                       "boruvka_minho_seq, single-threaded like the reference"},
+            "cpu_baseline": {"value": val, "unit": "edges/s", "cores": threads, "kind": "port",
+                             "sample": "per step, %d concurrent copies of the full graph, one per "
+                                       "host thread; the oracle's C restatement of "
+                                       "boruvka_minho_seq (sequential, like the reference)"
+                                       % threads},
             "e2e": {"value": val, "unit": "edges/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
