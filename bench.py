@@ -147,8 +147,10 @@ def measured_peak():
 # kernels whose roofline the bench reports: (library profiling tag, name,
 # algorithmic bytes per launch)
 ROOF_KERNELS = [
-    (0, "k_edge_tile (Boruvka contraction + fused min-edge)",
-     "8 B read per edge word + 8 B written per surviving edge"),
+    (0, "k_rounds (every Boruvka round of a weight phase in one persistent kernel)",
+     "per round: 8 B per edge word read + 8 B per surviving word written + 8 B per original "
+     "vertex (label read and written) + 24 B per supervertex (selection slot, successor, "
+     "new id)"),
     (4, "k_phase_csr (weight-phase edge build + first min-edge selection)",
      "12 B per vertex (row extent, label) + 5 B per CSR entry (dest, uint8 weight) "
      "+ 8 B per edge word written"),
@@ -158,7 +160,7 @@ ROOF_KERNELS = [
 def profiled_traffic(kernel):
     """DRAM bytes per launch of `kernel` from its committed ncu summary
     (profiles/<kernel>_knn16_1M.md; None when there is none)."""
-    name = {"k_edge_tile": "boruvka_edge_tile", "k_phase_csr": "boruvka_phase_csr"}.get(kernel)
+    name = {"k_rounds": "boruvka_rounds", "k_phase_csr": "boruvka_phase_csr"}.get(kernel)
     p = os.path.join(ROOT, "profiles", "%s_knn16_1M.md" % name) if name else ""
     if not p or not os.path.exists(p):
         return None
@@ -286,7 +288,7 @@ def run_ours(args):
         step()
     # ---- device-resident timed region ----
     barrier()
-    _lib.profile_enable(False)          # clears the launch counter; rounds run as CUDA graphs
+    _lib.profile_enable(False)          # clears the launch counter
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     with ClockSampler(local) as clk:
@@ -300,7 +302,7 @@ def run_ours(args):
     assert nm.value == V - 1
     t_ms = sum(a.elapsed_time(b) for a, b in ev)
     # ---- kernel roofline: a second pass with per-launch CUDA events ----
-    # (profiling drives the rounds from the host, so it stays out of the
+    # (profiling synchronizes after each timed launch, so it stays out of the
     # timed region above)
     _lib.profile_enable(True)
     p_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))

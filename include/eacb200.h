@@ -17,8 +17,8 @@
  *     never throw; outputs are undefined after an error;
  *   - functions whose work has data-dependent sizes (Boruvka, connected
  *     components, co-association, k-means, final clustering) synchronize
- *     `stream` a few times per call to read counters (Boruvka rounds loop on
- *     the device inside one CUDA graph per weight phase); the scans are
+ *     `stream` a few times per call to read counters (all Boruvka rounds of
+ *     a weight phase run inside one persistent kernel); the scans are
  *     asynchronous on `stream`;
  *   - entry points may be called from several host threads at once on
  *     different streams and workspaces (eacb_scan_excl_i32_noalloc excepted).
@@ -71,11 +71,22 @@ int eacb_workspace_status(void *ws, uintptr_t stream);
 /* Built-in profiling, off by default.  eacb_profile_enable(1) resets the
  * counters and turns on CUDA-event timing (on the launching stream) of the
  * tagged kernels; eacb_profile_read returns the number of kernels the
- * library launched since, and per tag (0 = Boruvka contraction tile,
- * 1 = scan, 2 = co-association rows, 3 = k-means labels; arrays of 8) the
- * total milliseconds, algorithmic bytes and launches. */
+ * library launched since, and per tag (0 = Boruvka round kernel, 1 = scan,
+ * 2 = co-association rows, 3 = k-means labels, 4 = Boruvka weight-phase
+ * builds; arrays of 8) the total milliseconds, algorithmic bytes and
+ * launches. */
 void eacb_profile_enable(int on);
 void eacb_profile_read(int64_t *launches, double *ms, double *bytes, int64_t *count);
+
+/* Test hooks of the Boruvka round kernel, process-wide, to be set between
+ * calls.  eacb_debug_set_round_cap: rounds a weight phase may run (0 = the
+ * built-in cap of 96); a graph that needs more returns
+ * EACB_ERR_NOT_CONVERGED, as an inconsistent one does at the built-in cap.
+ * eacb_debug_set_round_team: participants of the round kernel (0 =
+ * automatic, 1 = a single block, more = that many cooperative blocks, at
+ * most the number that can be resident); results do not depend on it. */
+void eacb_debug_set_round_cap(int rounds);
+void eacb_debug_set_round_team(int blocks);
 
 /* ------------------------------------------------------------------------
  * Exclusive prefix sum.
@@ -104,10 +115,12 @@ int eacb_scan_excl_i64(const int64_t *in, int64_t *out, int64_t n, int64_t init,
  * held on every GPU that loads the library until the process exits.  n may
  * not exceed EACB_SCAN_NOALLOC_MAX_N (returns EACB_ERR_WORKSPACE beyond it).
  * The first call on each device looks up that array's address
- * (cudaGetSymbolAddress; make this first call before any stream capture).
- * Calls share the array: calls that overlap on the GPU race, so serialise
- * them.  The call waits for the scan to finish and returns its device-side
- * status. */
+ * (cudaGetSymbolAddress; make this first call before any stream capture)
+ * and keeps it for the life of the process: do not call this entry point
+ * on a device after resetting it (cudaDeviceReset).  Calls share the array:
+ * calls that overlap on the GPU race, so serialise them.  Each call copies
+ * its device-side status to the host, synchronizes `stream` (so it returns
+ * only after the scan has finished) and returns that status. */
 #define EACB_SCAN_NOALLOC_MAX_N (((int64_t)1) << 28)
 int eacb_scan_excl_i32_noalloc(const int32_t *in, int32_t *out, int64_t n, int64_t init,
                                int64_t *d_total, uintptr_t stream);

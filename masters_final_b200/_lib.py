@@ -58,7 +58,8 @@ def load():
         "eacb_scan_excl_i32": (ctypes.c_int, [p, p, i64, i64, p, p, sz, p]),
         "eacb_scan_excl_i32_i64": (ctypes.c_int, [p, p, i64, i64, p, p, sz, p]),
         "eacb_scan_excl_i64": (ctypes.c_int, [p, p, i64, i64, p, p, sz, p]),
-        "eacb_debug_set_rounds": (None, [ctypes.c_int]),
+        "eacb_debug_set_round_cap": (None, [ctypes.c_int]),
+        "eacb_debug_set_round_team": (None, [ctypes.c_int]),
         "eacb_boruvka_workspace_size": (sz, [i32, i64]),
         "eacb_boruvka_mst": (ctypes.c_int, [p, p, ctypes.c_int, p, p, i32, i64, p, P64, p, sz, p]),
         "eacb_connected_components": (ctypes.c_int, [p, p, ctypes.c_int, p, p, i32, i64, p, P64,

@@ -16,13 +16,16 @@
 //    reference's connected-components numbering.  Lanes of a warp holding
 //    edges of the same supervertex are pre-reduced with a segmented shuffle
 //    scan, so one atomic is issued per run, not per edge.
-//  * Contraction is a single-pass, order-preserving stream compaction
-//    (decoupled look-back over 2048-edge tiles) fused with the NEXT round's
-//    min-edge selection: each edge is read once and written once per round.
+//  * All Boruvka rounds of a phase run in ONE persistent kernel (k_rounds):
+//    a cooperative grid whose blocks meet at bounded grid barriers, or a
+//    single block for small graphs.  Contraction is fused with the NEXT
+//    round's min-edge selection: each edge is read once and written at most
+//    once per round.
 //  * Mutual picks are broken towards the larger id like the reference; roots
 //    are found by a bounded pointer chase with path halving; supervertices are
-//    renumbered by an exclusive scan of the root flags (root order), which is
-//    the reference's numbering.
+//    renumbered in root order, which is the reference's numbering.
+//  * The MST grows by weight phases (Kruskal's prefix property), so heavy
+//    edges that lighter ones made internal are dropped by one filtering read.
 #include "eacb_common.cuh"
 #include "scan_impl.cuh"
 
@@ -127,28 +130,7 @@ constexpr int64_t kETile = (int64_t)kET * kEI;
 // Each source splits an edge into fetch() (independent global loads, issued
 // for all items of a thread before any is used) and resolve() (the dependent
 // work), so a thread keeps all its loads in flight at once.
-// (a) the current edge array: fetch the word, resolve its endpoints'
-//     supervertices (two gathers from the L2-resident label array)
-struct SrcEdges {
-    typedef uint64_t Raw;
-    const uint64_t *e;
-    const int32_t *label;
-    Pack pk;
-    uint32_t V0;
-    __device__ __forceinline__ void fetch(int64_t i, Raw &r) const { r = __ldcs(e + i); }
-    __device__ __forceinline__ bool resolve(const Raw &r, uint64_t &k, int32_t &su, int32_t &sv,
-                                            uint32_t &w) const
-    {
-        k = r;
-        if (pk.a(k) >= V0 || pk.b(k) >= V0) return false;   // dead words (never real edges)
-        su = label[pk.src(k)];
-        sv = label[pk.dst(k)];
-        w = pk.w(k);
-        return su != sv;
-    }
-};
-
-// (b) both directions of undirected keys (MST selection keys) below a weight cap
+// Both directions of undirected keys (MST selection keys) below a weight cap
 struct SrcForest {
     typedef uint64_t Raw;
     const uint64_t *keys;   // selection keys (w, a, b)
@@ -532,123 +514,154 @@ __device__ __forceinline__ void phase_stage(bool keep, uint64_t k, uint64_t *sta
     cnt += nb;
 }
 
+// identity: the first phase (every vertex its own root: no label is read,
+// and every entry is checked once for a destination out of range).
+// skip_root (device int, or null; -1 = none): a later phase skips the rows of
+// that root -- the giant component the earlier phases built -- and emits
+// both directions of each kept entry whose other end lies in it, so the
+// giant still sees every edge it has to another component (each such edge is
+// found once, from the row outside the giant).
 template <typename WT>
 __global__ void __launch_bounds__(kPhThreads)
 k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const WT *weight,
             int32_t V, int64_t E, int wbits, int lo, int hi, const int *dev_lohi, int slot,
-            const int32_t *label, Pack pk, uint64_t *eout, unsigned long long *cursor,
-            unsigned long long cap, unsigned long long *best, int *err)
+            int identity, const int32_t *skip_root, const int32_t *label, Pack pk,
+            uint64_t *eout, unsigned long long *cursor, unsigned long long cap,
+            unsigned long long *best, int *err)
 {
     if (dev_lohi) {
         lo = dev_lohi[2 * slot];
         hi = dev_lohi[2 * slot + 1];
     }
+    const int32_t skip = skip_root ? *skip_root : -1;
     __shared__ uint64_t stage_all[kPhWarps][kPhStage];
     __shared__ int64_t s_cnt[kPhWarps];
     __shared__ unsigned long long s_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint64_t *stage = stage_all[warp];
     const int64_t step = (int64_t)kPhWarps * 32;
-    // entry test: the candidate word of entry e of row u (supervertex lu)
-    auto test = [&](int64_t e, int64_t u, int32_t lu, uint64_t &k) -> bool {
-        const int32_t v = dest[e];
-        if (v < 0 || v >= V) {
-            set_err(err, DEV_BAD_INPUT);
-            return false;
+    auto root_of = [&](int32_t v) -> int32_t { return identity ? v : label[v]; };
+    // emits the kept entry u -> v (roots lu != lv): its word, offered to lu,
+    // and when v's root is the skipped giant, the reverse word, offered to it
+    auto emit = [&](bool keep, uint32_t w, int32_t u, int32_t v, int32_t lu, int32_t lv,
+                    int &cnt) {
+        const uint64_t k = keep ? pk.make(w, (uint32_t)u, (uint32_t)v) : 0ull;
+        phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
+        if (keep) min_if_lower(&best[lu], k >> 1);
+        if (skip >= 0) {
+            const bool rev = keep && lv == skip;
+            if (__any_sync(0xffffffffu, rev)) {
+                phase_stage(rev, k ^ 1ull, stage, cnt, eout, cursor, cap, err);
+                if (rev) min_if_lower(&best[skip], k >> 1);
+            }
         }
-        if (v == (int32_t)u) return false;
-        const uint32_t w = wword(weight[e]);
-        const int bk = (int)wbucket(w, wbits);
-        if (bk <= lo || bk > hi || label[v] == lu) return false;
-        k = pk.make(w, (uint32_t)u, (uint32_t)v);
-        return true;
     };
     for (int64_t r0 = (int64_t)blockIdx.x * step; r0 < V; r0 += (int64_t)gridDim.x * step) {
         const int64_t u0 = r0 + (int64_t)warp * 32;
         const int nrows = u0 >= V ? 0 : (int)(V - u0 < 32 ? V - u0 : 32);
         int64_t f = 0, d = 0;
         int32_t lu = 0;
+        bool live = false;
         if (lane < nrows) {
-            f = first[u0 + lane];
-            d = deg[u0 + lane];
-            if (f < 0 || d < 0 || f + d > E) {
-                set_err(err, DEV_BAD_INPUT);
-                f = 0;
-                d = 0;
+            lu = root_of((int32_t)(u0 + lane));
+            live = lu != skip;
+            if (live) {
+                f = first[u0 + lane];
+                d = deg[u0 + lane];
+                if (f < 0 || d < 0 || f + d > E) {
+                    set_err(err, DEV_BAD_INPUT);
+                    f = 0;
+                    d = 0;
+                }
             }
-            lu = label[u0 + lane];
         }
-        // rows back to back?  (row l + 1 starts where row l ends)
-        const int64_t f_next = __shfl_down_sync(0xffffffffu, f, 1);
-        const bool linked = lane + 1 >= nrows || f_next == f + d;
-        const int64_t e_begin = __shfl_sync(0xffffffffu, f, 0);
-        const int64_t e_end = nrows > 0 ? __shfl_sync(0xffffffffu, f + d, nrows - 1) : 0;
-        const bool flat = __all_sync(0xffffffffu, linked) && nrows > 0 &&
-                          e_end - e_begin < ((int64_t)1 << 30);
         int cnt = 0;
-        if (flat) {
-            const int32_t frel = (int32_t)(f - e_begin);      // row starts, warp-relative
-            // four 32-entry slices per step, the loads of all in flight together
-            constexpr int S = 4;
-            for (int64_t e0 = e_begin; e0 < e_end; e0 += 32 * S) {
-                int64_t e[S];
-                int r[S];
-                int32_t lr[S], v[S];
-                uint32_t w[S];
-                bool in[S];
+        if (__any_sync(0xffffffffu, live)) {
+            // rows back to back?  (row l + 1 starts where row l ends; a
+            // skipped row must not break the range, so it counts as empty
+            // only when the whole warp is flat over the live rows)
+            const int64_t f_next = __shfl_down_sync(0xffffffffu, f, 1);
+            const bool nl = __shfl_down_sync(0xffffffffu, live, 1);
+            const bool linked = lane + 1 >= nrows || !live || !nl || f_next == f + d;
+            const unsigned lmask = __ballot_sync(0xffffffffu, live);
+            const int lfirst = __ffs(lmask) - 1, llast = 31 - __clz(lmask);
+            const int64_t e_begin = __shfl_sync(0xffffffffu, f, lfirst);
+            const int64_t e_end = __shfl_sync(0xffffffffu, f + d, llast);
+            const bool flat = __all_sync(0xffffffffu, linked) && lmask == (nrows >= 32 ? 0xffffffffu : ((1u << nrows) - 1u)) &&
+                              e_end - e_begin < ((int64_t)1 << 30);
+            if (flat) {
+                const int32_t frel = (int32_t)(f - e_begin);      // row starts, warp-relative
+                // four 32-entry slices per step, the loads of all in flight together
+                constexpr int S = 4;
+                for (int64_t e0 = e_begin; e0 < e_end; e0 += 32 * S) {
+                    int64_t e[S];
+                    int r[S];
+                    int32_t lr[S], v[S];
+                    uint32_t w[S];
+                    bool in[S];
 #pragma unroll
-                for (int q = 0; q < S; ++q) {
-                    e[q] = e0 + 32 * q + lane;
-                    in[q] = e[q] < e_end;
-                    const int32_t erel = (int32_t)(e[q] - e_begin);
-                    // row of entry e: the last row starting at or before e
-                    int rr = 0;
+                    for (int q = 0; q < S; ++q) {
+                        e[q] = e0 + 32 * q + lane;
+                        in[q] = e[q] < e_end;
+                        const int32_t erel = (int32_t)(e[q] - e_begin);
+                        // row of entry e: the last row starting at or before e
+                        int rr = 0;
 #pragma unroll
-                    for (int st = 16; st >= 1; st >>= 1) {
-                        const int c = rr + st;
-                        const int32_t fs = __shfl_sync(0xffffffffu, frel, c & 31);
-                        if (c < nrows && fs <= erel) rr = c;
-                    }
-                    r[q] = rr;
-                    lr[q] = __shfl_sync(0xffffffffu, lu, rr);
-                    v[q] = in[q] ? dest[e[q]] : -1;
-                    w[q] = in[q] ? wword(weight[e[q]]) : 0u;
-                }
-                bool cand[S];
-                int32_t lv[S];
-#pragma unroll
-                for (int q = 0; q < S; ++q) {
-                    cand[q] = false;
-                    if (in[q]) {
-                        if (v[q] < 0 || v[q] >= V) {
-                            set_err(err, DEV_BAD_INPUT);
-                        } else if (v[q] != (int32_t)(u0 + r[q])) {
-                            const int bk = (int)wbucket(w[q], wbits);
-                            cand[q] = bk > lo && bk <= hi;
+                        for (int st = 16; st >= 1; st >>= 1) {
+                            const int c = rr + st;
+                            const int32_t fs = __shfl_sync(0xffffffffu, frel, c & 31);
+                            if (c < nrows && fs <= erel) rr = c;
                         }
+                        r[q] = rr;
+                        lr[q] = __shfl_sync(0xffffffffu, lu, rr);
+                        v[q] = in[q] ? dest[e[q]] : -1;
+                        w[q] = in[q] ? wword(weight[e[q]]) : 0u;
                     }
-                    lv[q] = cand[q] ? label[v[q]] : 0;
-                }
+                    bool cand[S];
+                    int32_t lv[S];
 #pragma unroll
-                for (int q = 0; q < S; ++q) {
-                    const bool keep = cand[q] && lv[q] != lr[q];
-                    const uint64_t k =
-                        keep ? pk.make(w[q], (uint32_t)(u0 + r[q]), (uint32_t)v[q]) : 0ull;
-                    phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
-                    if (keep) min_if_lower(&best[lr[q]], k >> 1);
+                    for (int q = 0; q < S; ++q) {
+                        cand[q] = false;
+                        if (in[q]) {
+                            if (v[q] < 0 || v[q] >= V) {
+                                set_err(err, DEV_BAD_INPUT);
+                            } else if (v[q] != (int32_t)(u0 + r[q])) {
+                                const int bk = (int)wbucket(w[q], wbits);
+                                cand[q] = bk > lo && bk <= hi;
+                            }
+                        }
+                        lv[q] = cand[q] ? root_of(v[q]) : 0;
+                    }
+#pragma unroll
+                    for (int q = 0; q < S; ++q)
+                        emit(cand[q] && lv[q] != lr[q], w[q], (int32_t)(u0 + r[q]), v[q], lr[q],
+                             lv[q], cnt);
                 }
-            }
-        } else {
-            for (int rr = 0; rr < nrows; ++rr) {
-                const int64_t fr = __shfl_sync(0xffffffffu, f, rr);
-                const int64_t dr = __shfl_sync(0xffffffffu, d, rr);
-                const int32_t lr = __shfl_sync(0xffffffffu, lu, rr);
-                for (int64_t e0 = fr; e0 < fr + dr; e0 += 32) {
-                    const int64_t e = e0 + lane;
-                    uint64_t k = 0;
-                    const bool keep = e < fr + dr && test(e, u0 + rr, lr, k);
-                    phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
-                    if (keep) min_if_lower(&best[lr], k >> 1);
+            } else {
+                for (int rr = 0; rr < nrows; ++rr) {
+                    if (!((lmask >> rr) & 1u)) continue;
+                    const int64_t fr = __shfl_sync(0xffffffffu, f, rr);
+                    const int64_t dr = __shfl_sync(0xffffffffu, d, rr);
+                    const int32_t lr = __shfl_sync(0xffffffffu, lu, rr);
+                    const int32_t u = (int32_t)(u0 + rr);
+                    for (int64_t e0 = fr; e0 < fr + dr; e0 += 32) {
+                        const int64_t e = e0 + lane;
+                        bool cand = false;
+                        int32_t v = -1, lv = 0;
+                        uint32_t w = 0;
+                        if (e < fr + dr) {
+                            v = dest[e];
+                            if (v < 0 || v >= V) {
+                                set_err(err, DEV_BAD_INPUT);
+                            } else if (v != u) {
+                                w = wword(weight[e]);
+                                const int bk = (int)wbucket(w, wbits);
+                                cand = bk > lo && bk <= hi;
+                                if (cand) lv = root_of(v);
+                            }
+                        }
+                        emit(cand && lv != lr, w, u, v, lr, lv, cnt);
+                    }
                 }
             }
         }
@@ -659,6 +672,50 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
             for (int i = lane; i < cnt; i += 32) eout[at + i] = stage[i];
         }
         __syncthreads();          // staging and s_cnt are reused by the next step
+    }
+}
+
+// The root holding most vertices (from a strided sample of 2048 vertices, in
+// a shared-memory count table), or -1 when none holds a quarter of the
+// sample: the rows a later weight phase may skip.
+constexpr int kGiantSample = 2048;
+__global__ void __launch_bounds__(1024)
+k_pick_giant(const int32_t *label, int64_t V0, int32_t *out)
+{
+    constexpr int T = 2 * kGiantSample;
+    __shared__ int32_t key[T];
+    __shared__ int32_t cnt[T];
+    __shared__ unsigned long long best;
+    for (int i = threadIdx.x; i < T; i += blockDim.x) {
+        key[i] = -1;
+        cnt[i] = 0;
+    }
+    if (threadIdx.x == 0) best = 0ull;
+    __syncthreads();
+    const int64_t n = V0 < kGiantSample ? V0 : kGiantSample;
+    for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+        const int32_t r = label[(j * V0) / n];
+        unsigned slot = ((uint32_t)r * 2654435761u) % T;
+        for (int probe = 0; probe < T; ++probe) {
+            int32_t k = key[slot];
+            if (k == -1) {
+                k = atomicCAS(&key[slot], -1, r);
+                if (k == -1) k = r;
+            }
+            if (k == r) {
+                atomicAdd(&cnt[slot], 1);
+                break;
+            }
+            slot = (slot + 1) % T;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < T; i += blockDim.x)
+        if (cnt[i]) atomicMax(&best, ((unsigned long long)cnt[i] << 32) | (uint32_t)key[i]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int64_t c = (int64_t)(best >> 32);
+        *out = (n > 0 && 4 * c >= n) ? (int32_t)(uint32_t)best : -1;
     }
 }
 
@@ -877,13 +934,16 @@ __host__ __device__ static int phase_ranges(const unsigned long long *hist, cons
 // The weight phases of an MST on the device (no host read): ranges (lo, hi]
 // at cumulative fractions 1/8, 1/2, 1 of the histogram, one slot each in
 // lohi (an unused slot holds the empty range (255, 255]).
-constexpr int kPhaseSlots = 3;
+constexpr int kPhaseSlots = 2;
 __global__ void k_phase_plan(const unsigned long long *hist, int *lohi)
 {
+    __shared__ unsigned long long h[256];
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) h[b] = hist[b];
+    __syncthreads();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const double fracs[kPhaseSlots] = {0.125, 0.5, 1.0};
+    const double fracs[kPhaseSlots] = {0.25, 1.0};
     int lo[8], hi[8];
-    const int np = phase_ranges(hist, fracs, kPhaseSlots, lo, hi);
+    const int np = phase_ranges(h, fracs, kPhaseSlots, lo, hi);
     for (int q = 0; q < kPhaseSlots; ++q) {
         lohi[2 * q] = q < np ? lo[q] : 255;
         lohi[2 * q + 1] = q < np ? hi[q] : 255;
@@ -897,171 +957,654 @@ __global__ void k_iota(int32_t *a, int64_t n)
         a[i] = (int32_t)i;
 }
 
+// Every vertex its own root (parent) and its own successor (color): a root
+// that no round visits keeps color[s] == s.
+__global__ void k_iota2(int32_t *a, int32_t *b, int64_t n)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        a[i] = (int32_t)i;
+        b[i] = (int32_t)i;
+    }
+}
+
 constexpr int kMaxRounds = 96;   // Boruvka rounds per phase (halving: 96 is never reached)
 
-// Round state kept on the device, so that a round needs no host value and
-// the rounds can loop inside one CUDA graph (see Engine::run):
+// Round state kept on the device (int64 words), so that the phases of an MST
+// can be queued back to back without a host read:
 enum : int {
-    C_E_NEXT = 0,     // edges after this round's contraction (filter total)
-    C_V_NEXT = 1,     // supervertices after this round (root-scan total)
-    C_EMIT = 2,       // forest edges emitted this round (emit-scan total)
+    C_V = 0,          // supervertices at the start of the next round
+    C_E = 1,          // edge words in the round kernel's input buffer
+    C_NMST = 2,       // forest edges emitted so far (all phases)
     C_CURSOR = 3,     // phase-build output cursor
-    C_V = 4,          // supervertices at the start of the round
-    C_E = 5,          // edges at the start of the round
-    C_NMST = 6,       // forest edges emitted so far (all phases)
-    C_ROUNDS = 7,     // rounds run in this phase
-    C_DONE = 8,       // 1 once the phase has converged
-    C_ROUNDS_ALL = 9, // rounds run since the engine's reset (all phases)
+    C_ROUNDS = 4,     // rounds run by the last round kernel
+    C_DONE = 5,       // how the last round kernel ended (see k_rounds)
+    C_ROUNDS_ALL = 6, // rounds run since the engine's reset (all phases)
+    C_EBUF = 7,       // edge buffer holding the last round's survivors (0 or 1)
+    C_AUX0 = 8,       // scratch totals of single-pass kernels
+    C_AUX1 = 9,
     C_COUNT = 16
 };
 
-// successor of each supervertex from its selected key
-template <int MODE>
-__global__ void k_select(const unsigned long long *best, int32_t *succ, const int64_t *dV,
-                         const int32_t *label, Pack pk)
-{
-    const int64_t V = *dV;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
-         s += (int64_t)gridDim.x * blockDim.x) {
-        uint64_t b = best[s];
-        int32_t t = (int32_t)s;
-        if (b != kNone) {
-            if (MODE == SEL_CC) {
-                t = (int32_t)(uint32_t)b;
-            } else {
-                int32_t la = label[pk.sel_a(b)], lb = label[pk.sel_b(b)];
-                t = (la == (int32_t)s) ? lb : la;
-            }
-        }
-        succ[s] = t;
-    }
-}
-
-// Look-back state of the next single-pass kernel, cleared by the kernel
-// before it (one launch fewer per scan).
-__device__ __forceinline__ void clear_lookback(uint64_t *status, int64_t n_status, int *counter)
-{
-    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    for (int64_t i = t0; i < n_status; i += (int64_t)gridDim.x * blockDim.x) status[i] = 0;
-    if (t0 == 0) *counter = 0;
-}
-
-// mutual picks: the smaller id drops its edge (MyML/MyML/graph/mst.py:283-305)
-__global__ void k_mirror(const int32_t *succ, int32_t *color, int32_t *emit, const int64_t *dV,
-                         uint64_t *status, int64_t n_status, int *counter)
-{
-    const int64_t V = *dV;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
-         s += (int64_t)gridDim.x * blockDim.x) {
-        int32_t t = succ[s];
-        bool has = t != (int32_t)s;
-        bool drop = has && succ[t] == (int32_t)s && (int32_t)s < t;
-        color[s] = (has && !drop) ? t : (int32_t)s;
-        if (emit) emit[s] = (has && !drop) ? 1 : 0;
-    }
-    clear_lookback(status, n_status, counter);
-}
-
-// One pass per supervertex s: (MST) emits its selected edge at its scanned
-// position, appended after the forest edges of earlier rounds; finds its root
-// by pointer chasing with path halving, bounded (a non-forest errors); flags
-// roots for the renumbering scan.  A halving step replaces c's parent p by
-// its grandparent g only if c still points at p (compare-and-swap): a plain
-// store could overwrite the root that c's own thread already stored, leaving
-// c on a non-root.  s is a root exactly when its own chase ends at s.
-__global__ void k_jump(int32_t *color, const int64_t *dV, int *err,
-                       const unsigned long long *best, int32_t *flag, const int32_t *pos,
-                       uint64_t *out, const int64_t *d_base, uint64_t *status, int64_t n_status,
-                       int *counter)
-{
-    const int64_t V = *dV;
-    uint64_t *o = out ? out + *d_base : nullptr;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < V;
-         s += (int64_t)gridDim.x * blockDim.x) {
-        if (o && flag[s]) o[pos[s]] = best[s];
-        int32_t c = color[s];
-        int64_t guard = 0;
-        while (true) {
-            int32_t p = color[c];
-            if (p == c) break;
-            int32_t g = color[p];
-            if (g != p) atomicCAS(&color[c], p, g);
-            c = g;
-            if (++guard > (int64_t)V + 64) {
-                set_err(err, DEV_CHASE_LIMIT);
-                break;
-            }
-        }
-        color[s] = c;
-        flag[s] = c == (int32_t)s;
-    }
-    clear_lookback(status, n_status, counter);
-}
-
-// Relabels every original vertex to its new supervertex id, and clears the
-// next round's selection (Vn supervertices) and the contraction's look-back
-// state.
-__global__ void k_relabel(int32_t *label, const int32_t *color, const int32_t *newid, int64_t V0,
-                          unsigned long long *best, const int64_t *dVn, uint64_t *status,
-                          int64_t n_status, int *counter, int64_t *d_count)
-{
-    const int64_t Vn = *dVn;
-    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t x = t0; x < V0; x += stride) label[x] = newid[color[label[x]]];
-    for (int64_t x = t0; x < Vn; x += stride) best[x] = kNone;
-    clear_lookback(status, n_status, counter);
-    if (t0 == 0) *d_count = 0;
-}
-
 // Start of a phase queued without a host read: its edge count is the
-// build's cursor, its supervertex count the previous phase's result (V0
-// for the first phase).
+// build's cursor, its supervertex count the previous phase's result (V0 for
+// the first phase).
 __global__ void k_phase_begin(int64_t *cnt, int64_t V0, int first_phase)
 {
     if (threadIdx.x == 0) {
         if (first_phase) cnt[C_V] = V0;
         cnt[C_E] = cnt[C_CURSOR];
-        cnt[C_ROUNDS] = 0;
-        cnt[C_DONE] = 0;
     }
 }
 
-__global__ void k_round_begin(int64_t *cnt, int64_t V, int64_t E)
+__global__ void k_set_sizes(int64_t *cnt, int64_t V, int64_t E)
 {
     if (threadIdx.x == 0) {
         cnt[C_V] = V;
         cnt[C_E] = E;
-        cnt[C_ROUNDS] = 0;
-        cnt[C_DONE] = 0;
     }
 }
 
-// End of a round: advance the sizes and decide whether another round runs.
-// cnt[C_DONE]: 0 = continue, 1 = converged (one supervertex or no edge
-// left), 2 = no contraction (an error), 3 = round limit, 4 = device error.
-// Inside a graph, the loop condition is cleared when the phase is done.
-// A phase that stops without converging (no contraction, or the round limit
-// when that limit is not a deliberate stop) also raises DEV_CHASE_LIMIT, so
-// phases queued after it report the failure at the end.
-__global__ void k_round_end(int64_t *cnt, int is_mst, int max_rounds, int *err,
-                            cudaGraphConditionalHandle h, int use_handle)
+// ---------------------------------------------------------------------------
+// Boruvka rounds: all rounds of a phase in ONE persistent kernel.
+//
+// Supervertices are named by an original vertex, their root: `parent` is a
+// union-find forest over the original vertices (a root points to itself), so
+// a round never renumbers anything and never sweeps all original vertices;
+// an edge endpoint or a key endpoint finds its supervertex by following
+// parent pointers (and shortens the path it walked).  Only the ACTIVE roots
+// -- those with an edge to another supervertex -- are visited, from a list
+// kept in increasing id order.
+//
+// The participants are either every block of a cooperative grid (all blocks
+// resident at once, so they may wait on one another) or a single block.
+// Each participant owns a contiguous chunk of the original vertices (its
+// part of the active list) and a contiguous segment of the phase's edge
+// words; both shrink in place.  Between the steps of a round the
+// participants meet at a barrier: a bounded spin on a generation word for the
+// grid, __syncthreads for one block.  Once few active roots and edges are
+// left, the grid's other blocks leave and block 0 runs the remaining rounds
+// alone for every participant's chunk and segment (no grid barriers).
+// A round is
+//   A. per active root s: its successor t (the root of the other end of its
+//      selected key); a mutual pick (t's successor is s) is broken towards
+//      the larger id, so the smaller one stays a root
+//      (MyML/MyML/graph/mst.py:283-305); color[s] = t, or s.
+//   B. in list order: each non-root emits its key as a forest edge (slots in
+//      root-id order, from the participants' counts), finds its new root
+//      (bounded chase with compare-and-swap path halving over color) and
+//      points its parent there; the roots that still have an edge stay in the
+//      list, and their selection slots are cleared.
+//   D. contraction fused with the next round's minimum-edge selection: each
+//      edge word whose endpoints now have different roots stays in its
+//      segment (compacted in place: a tile's words are in registers before
+//      any of the tile's survivors is written, and survivors never move past
+//      their tile) and is offered to its source root's slot (one atomicMin
+//      per run of equal source in a warp).  Edge order does not matter:
+//      selection uses total orders, so every result is independent of it.
+// Three barriers per round.  After the last one every participant reads the
+// same sizes and takes the same decision to stop:
+//   C_DONE = 1 converged (no edge left), 2 no contraction (not a valid
+//   graph), 3 round cap, 4 a device error.
+// Root ids keep the reference's choices: its renumbering is order-preserving,
+// so "smaller id" and "smallest destination" compare the same way, and its
+// final component number is the rank of the root id (k_rank_roots).
+// The steps handle several elements per thread at a time with all loads of
+// one level issued together: they are chains of dependent gathers, so the
+// independent chains in flight, not bandwidth, set their speed.
+// ---------------------------------------------------------------------------
+constexpr int kRT = 1024;                       // round-kernel threads per block
+constexpr int kRItems = 4;                      // edge words per thread per tile
+constexpr int kRV = 4;                          // vertices per thread per step
+constexpr int64_t kRTile = (int64_t)kRT * kRItems;
+constexpr int kRWarps = kRT / 32;
+constexpr int kMaxTeam = 148 * 8;               // participants (blocks) at most
+constexpr long long kBarrierSpins = 1ll << 21;  // about a second of waiting
+constexpr int64_t kSoloActive = 1024;           // block 0 alone below these sizes
+constexpr int64_t kSoloEdges = 8192;
+constexpr int kFindLimit = 1 << 20;             // parent-chain steps (a forest is shorter)
+
+struct GridBarrier {
+    unsigned count;
+    unsigned gen;
+};
+
+// Grid-wide barrier of a cooperative launch.  Thread 0 of each block arrives
+// on a counter; the last to arrive resets it and advances the generation the
+// others wait on.  The wait gives up after about a second (DEV_SPIN_LIMIT),
+// or as soon as any block has raised an error, so a block that left early
+// never holds the others.  Returns false when it gave up.  The fences order
+// each block's writes before its arrival and its reads after the wait; the
+// data exchanged between blocks is read with L1-bypassing loads.
+__device__ __forceinline__ bool grid_barrier(GridBarrier *b, int *err)
 {
-    if (threadIdx.x != 0) return;
-    const int64_t V = cnt[C_V], Vn = cnt[C_V_NEXT], En = cnt[C_E_NEXT];
-    if (is_mst) cnt[C_NMST] += cnt[C_EMIT];
-    const int64_t r = ++cnt[C_ROUNDS];
-    ++cnt[C_ROUNDS_ALL];
-    int64_t done = 0;
-    if (*(volatile const int *)err) done = 4;
-    else if (Vn <= 1 || En == 0) done = 1;
-    else if (Vn >= V) done = 2;
-    else if (r >= max_rounds) done = 3;
-    if (done == 2 || (done == 3 && max_rounds >= kMaxRounds)) set_err(err, DEV_CHASE_LIMIT);
-    cnt[C_DONE] = done;
-    cnt[C_V] = Vn;
-    cnt[C_E] = En;
-    if (use_handle) cudaGraphSetConditional(h, done ? 0u : 1u);
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *vgen = &b->gen;
+        const unsigned g = *vgen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
+            atomicExch(&b->count, 0u);
+            __threadfence();
+            atomicAdd(&b->gen, 1u);
+        } else {
+            long long spins = 0;
+            while (*vgen == g) {
+                if (*(volatile int *)err) {
+                    ok = 0;
+                    break;
+                }
+                if (++spins > kBarrierSpins) {
+                    set_err(err, DEV_SPIN_LIMIT);
+                    ok = 0;
+                    break;
+                }
+                if (spins > 256) __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+struct RoundArgs {
+    Pack pk;
+    int64_t V0;
+    uint64_t *e;                  // edge words of the phase (compacted per segment)
+    int32_t *parent;              // V0: union-find parent (a root points to itself)
+    unsigned long long *best;     // V0: selection slot per root
+    int32_t *color;               // V0: successor, then new root, per active root
+    int32_t *act;                 // V0: active roots, per participant chunk
+    uint64_t *mst;                // forest keys, appended at cnt[C_NMST] (MST mode)
+    int32_t *part;                // 2 x kMaxTeam: per participant (emits, merges)
+    int32_t *alen;                // kMaxTeam: active roots per participant
+    int64_t *seg;                 // kMaxTeam: edge words per participant segment
+    int64_t *cnt;                 // C_* round state
+    int64_t *trace;               // 3 x kMaxRounds: (V, E, active) per round
+    GridBarrier *bar;
+    int *err;
+    int max_rounds;
+};
+
+// Roots of N vertices at once (all parent loads of one level issued
+// together); each vertex whose first parent was not its root is pointed at
+// the root (a benign race: every writer writes the same root).  Negative
+// ids (empty lanes) are left alone: they must not all walk and rewrite the
+// path of one real vertex.
+// The parent loads may be served by L1: late rounds send most finds to the
+// few roots left, and L2-only loads of those few lines from every SM
+// serialise (a 20x slower contraction measured on a 16-NN graph).  The
+// entries a round rewrites (merged roots, step B) were written before the
+// barrier that precedes the finds, whose acquire fence orders the later
+// loads after them; within a step the only writes are path compressions,
+// so a stale value is an older ancestor and the walk still ends at the root.
+template <int N>
+__device__ __forceinline__ void find_batch(int32_t *parent, int32_t (&x)[N], int *err)
+{
+    int32_t r[N], first[N];
+    bool go[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        r[i] = x[i] >= 0 ? parent[x[i]] : x[i];
+        first[i] = r[i];
+        go[i] = r[i] != x[i];
+    }
+    for (int step = 0;; ++step) {
+        int32_t up[N];
+        bool any = false;
+#pragma unroll
+        for (int i = 0; i < N; ++i) up[i] = go[i] ? parent[r[i]] : r[i];
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            if (go[i] && up[i] != r[i]) {
+                r[i] = up[i];
+                any = true;
+            } else {
+                go[i] = false;
+            }
+        }
+        if (!any) break;
+        if (step > kFindLimit) {
+            set_err(err, DEV_CHASE_LIMIT);
+            break;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        if (first[i] != x[i] && first[i] != r[i]) parent[x[i]] = r[i];
+        x[i] = r[i];
+    }
+}
+
+// Successors of up to kRV active roots at once (s[i] < 0: none): the root of
+// the other end of each selected key, or the root itself when it selected
+// nothing.
+template <int MODE>
+__device__ __forceinline__ void succ_batch(const RoundArgs &a, const int32_t (&s)[kRV],
+                                           int32_t (&t)[kRV])
+{
+    uint64_t b[kRV];
+#pragma unroll
+    for (int i = 0; i < kRV; ++i) b[i] = s[i] >= 0 ? __ldcg(a.best + s[i]) : kNone;
+    if constexpr (MODE == SEL_CC) {
+#pragma unroll
+        for (int i = 0; i < kRV; ++i) t[i] = b[i] == kNone ? s[i] : (int32_t)(uint32_t)b[i];
+    } else {
+    int32_t e[2 * kRV];
+#pragma unroll
+    for (int i = 0; i < kRV; ++i) {
+        const bool ok = b[i] != kNone;
+        e[2 * i] = ok ? (int32_t)a.pk.sel_a(b[i]) : -1;
+        e[2 * i + 1] = ok ? (int32_t)a.pk.sel_b(b[i]) : -1;
+    }
+    find_batch<2 * kRV>(a.parent, e, a.err);
+#pragma unroll
+    for (int i = 0; i < kRV; ++i)
+        t[i] = b[i] == kNone ? s[i] : (e[2 * i] == s[i] ? e[2 * i + 1] : e[2 * i]);
+    }
+}
+
+template <int MODE, bool GRID>
+__global__ void __launch_bounds__(kRT, 1)
+k_rounds(RoundArgs a)
+{
+    __shared__ int s_off[kRItems][kRWarps];
+    __shared__ int s_base;
+    __shared__ int s_err;
+    const int64_t P = GRID ? (int64_t)gridDim.x : 1, p = GRID ? (int64_t)blockIdx.x : 0;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    bool solo = !GRID;                  // one block does all the work
+    int64_t Pe = P;                     // participants whose chunks and segments are in use
+    auto sync = [&]() -> bool {
+        if (!solo) return grid_barrier(a.bar, a.err);
+        __syncthreads();
+        return true;
+    };
+    int64_t V = __ldcg(a.cnt + C_V), E = __ldcg(a.cnt + C_E);
+    int64_t nmst = __ldcg(a.cnt + C_NMST);
+    const int64_t E0 = E;
+    const int64_t seg_stride = (E0 + P - 1) / P;     // edge segment of participant q
+    const int64_t vchunk = (a.V0 + P - 1) / P;       // vertex chunk of participant q
+    auto ebase = [&](int64_t q) { return min(E0, q * seg_stride); };
+    auto vbase = [&](int64_t q) { return min(a.V0, q * vchunk); };
+
+    // ---- active list: the roots with a selection, in id order -------------
+    for (int64_t q = solo ? 0 : p; q < (solo ? P : p + 1); ++q) {
+        const int64_t v0 = vbase(q), v1 = min(a.V0, v0 + vchunk);
+        int64_t kept = 0;
+        for (int64_t xb = v0; xb < v1; xb += kRT) {
+            const int64_t x = xb + tid;
+            const bool in = x < v1;
+            const bool on = in && __ldcg(a.parent + x) == (int32_t)x && __ldcg(a.best + x) != kNone;
+            int64_t ttot;
+            const int64_t ex = block_excl_sum_shfl<kRT>(on ? 1 : 0, ttot);
+            if (on) a.act[v0 + kept + ex] = (int32_t)x;
+            kept += ttot;
+        }
+        const int64_t e0 = ebase(q);
+        if (tid == 0) {
+            a.alen[q] = (int32_t)kept;
+            a.seg[q] = min(E0, e0 + seg_stride) - e0;
+        }
+    }
+    if (tid == 0) s_err = *(volatile int *)a.err;
+    __syncthreads();
+    int round = 0, done = s_err ? 4 : ((E == 0 || V <= 1) ? 1 : 0);
+    if (!done && !sync()) done = 4;
+    int64_t Aact = 0;                                 // active roots this round
+    if (!done) {
+        int64_t x = 0;
+        for (int64_t j = tid; j < P; j += kRT) x += __ldcg(a.alen + j);
+        block_excl_sum_shfl<kRT>(x, Aact);
+    }
+    while (!done) {
+        const int64_t q0 = solo ? 0 : p, q1 = solo ? Pe : p + 1;
+        // ---- A: successors, mutual picks, per-participant counts ---------
+        for (int64_t q = q0; q < q1; ++q) {
+            const int32_t *al = a.act + vbase(q);
+            const int64_t n = __ldcg(a.alen + q);
+            int64_t mine = 0;                   // (forest edges << 32) | merges
+            for (int64_t ib = tid; ib < n; ib += (int64_t)kRT * kRV) {
+                int32_t s[kRV], t[kRV], tt[kRV], m[kRV];
+#pragma unroll
+                for (int i = 0; i < kRV; ++i) {
+                    const int64_t j = ib + (int64_t)i * kRT;
+                    s[i] = j < n ? __ldcg(al + j) : -1;
+                }
+                succ_batch<MODE>(a, s, t);
+                // mutual pick: only a smaller s with a successor needs t's
+#pragma unroll
+                for (int i = 0; i < kRV; ++i) m[i] = (s[i] >= 0 && s[i] < t[i]) ? t[i] : -1;
+                succ_batch<MODE>(a, m, tt);
+#pragma unroll
+                for (int i = 0; i < kRV; ++i) {
+                    if (s[i] < 0) continue;
+                    const bool keep = t[i] != s[i] && !(m[i] >= 0 && tt[i] == s[i]);
+                    a.color[s[i]] = keep ? t[i] : s[i];
+                    mine += keep ? ((MODE == SEL_MST ? (1ll << 32) : 0ll) | 1ll) : 0ll;
+                }
+            }
+            int64_t btot;
+            block_excl_sum_shfl<kRT>(mine, btot);
+            if (tid == 0) {
+                a.part[q] = (int32_t)(btot >> 32);             // forest edges
+                a.part[kMaxTeam + q] = (int32_t)(btot & 0xffffffffll);   // merges
+            }
+        }
+        if (!sync()) break;
+
+        // ---- B: forest edges, new roots, the next active list -----------
+        int64_t merges = 0, epre = 0;           // all merges; forest edges before q0
+        {
+            int64_t xp = 0, mg = 0;
+            for (int64_t j = tid; j < Pe; j += kRT) {
+                mg += __ldcg(a.part + kMaxTeam + j);
+                if (j < q0) xp += __ldcg(a.part + j);
+            }
+            block_excl_sum_shfl<kRT>(mg, merges);
+            block_excl_sum_shfl<kRT>(xp, epre);
+        }
+        for (int64_t q = q0; q < q1; ++q) {
+            int32_t *al = a.act + vbase(q);
+            const int64_t n = __ldcg(a.alen + q);
+            int64_t kept = 0;
+            for (int64_t base = 0; base < n; base += (int64_t)kRT * kRV) {
+                // thread tid takes kRV consecutive entries, so the block scans
+                // keep list order
+                int32_t s[kRV], c[kRV];
+                bool root[kRV], act[kRV], stay[kRV];
+                int64_t fl = 0;                 // (forest edges << 32) | staying roots
+                const int64_t jb = base + (int64_t)tid * kRV;
+#pragma unroll
+                for (int i = 0; i < kRV; ++i) {
+                    const bool in = jb + i < n;
+                    s[i] = in ? __ldcg(al + jb + i) : 0;
+                }
+#pragma unroll
+                for (int i = 0; i < kRV; ++i) {
+                    const bool in = jb + i < n;
+                    c[i] = in ? __ldcg(a.color + s[i]) : 0;
+                    root[i] = in && c[i] == s[i];
+                    act[i] = in && !root[i];
+                    // a root stays active only while it has an edge
+                    stay[i] = root[i] && __ldcg(a.best + s[i]) != kNone;
+                    fl += ((act[i] && MODE == SEL_MST) ? (1ll << 32) : 0ll) | (stay[i] ? 1ll : 0ll);
+                }
+                int64_t ttot;
+                int64_t ex = block_excl_sum_shfl<kRT>(fl, ttot);
+                __syncthreads();                // every entry of the tile is read
+                int64_t ep = epre + (ex >> 32), kp = kept + (ex & 0xffffffffll);
+#pragma unroll
+                for (int i = 0; i < kRV; ++i) {
+                    if (stay[i]) al[kp++] = s[i];
+                    if (act[i] && MODE == SEL_MST) a.mst[nmst + ep++] = __ldcg(a.best + s[i]);
+                }
+                // new roots of the non-roots: chases interleaved
+                for (int64_t guard = 0;; ++guard) {
+                    bool any = false;
+                    int32_t up[kRV], g[kRV];
+#pragma unroll
+                    for (int i = 0; i < kRV; ++i) up[i] = act[i] ? __ldcg(a.color + c[i]) : 0;
+#pragma unroll
+                    for (int i = 0; i < kRV; ++i) {
+                        if (act[i] && up[i] == c[i]) {
+                            act[i] = false;
+                            a.color[s[i]] = c[i];
+                            a.parent[s[i]] = c[i];
+                        }
+                        g[i] = act[i] ? __ldcg(a.color + up[i]) : 0;
+                    }
+#pragma unroll
+                    for (int i = 0; i < kRV; ++i) {
+                        if (!act[i]) continue;
+                        if (g[i] != up[i]) atomicCAS(a.color + c[i], up[i], g[i]);
+                        c[i] = g[i];
+                        any = true;
+                    }
+                    if (!any) break;
+                    if (guard > V + 64) {
+                        set_err(a.err, DEV_CHASE_LIMIT);
+                        break;
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < kRV; ++i)
+                    if (stay[i]) a.best[s[i]] = kNone;
+                kept += ttot & 0xffffffffll;
+                epre += ttot >> 32;
+            }
+            if (tid == 0) a.alen[q] = (int32_t)kept;
+        }
+        if (!sync()) break;
+
+        // ---- D: contraction of the segments, in place ---------------------
+        for (int64_t q = q0; q < q1; ++q) {
+            uint64_t *seg = a.e + ebase(q);
+            const int64_t elen = __ldcg(a.seg + q);
+            int64_t out = 0;                    // survivors written so far
+            for (int64_t base = 0; base < elen; base += kRTile) {
+                uint64_t k[kRItems];
+#pragma unroll
+                for (int it = 0; it < kRItems; ++it) {
+                    const int64_t i = base + (int64_t)it * kRT + tid;
+                    k[it] = i < elen ? __ldcg(seg + i) : kNone;
+                }
+                // dead words (self loops left by a CSR load) have a == b
+                int32_t ep[2 * kRItems];
+                bool ok[kRItems];
+#pragma unroll
+                for (int it = 0; it < kRItems; ++it) {
+                    ok[it] = k[it] != kNone && a.pk.a(k[it]) < (uint64_t)a.V0 &&
+                             a.pk.b(k[it]) < (uint64_t)a.V0;
+                    ep[2 * it] = ok[it] ? (int32_t)a.pk.src(k[it]) : -1;
+                    ep[2 * it + 1] = ok[it] ? (int32_t)a.pk.dst(k[it]) : -2;
+                }
+                find_batch<2 * kRItems>(a.parent, ep, a.err);
+                bool keep[kRItems];
+                unsigned bal[kRItems];
+#pragma unroll
+                for (int it = 0; it < kRItems; ++it) {
+                    const int32_t su = ep[2 * it], sv = ep[2 * it + 1];
+                    keep[it] = ok[it] && su != sv;
+                    bal[it] = __ballot_sync(0xffffffffu, keep[it]);
+                    if (lane == 0) s_off[it][warp] = __popc(bal[it]);
+                    const uint64_t sel = MODE == SEL_MST
+                                             ? (k[it] >> 1)
+                                             : (((uint64_t)a.pk.w(k[it]) << 32) | (uint32_t)sv);
+                    seg_min_atomic(keep[it], su, sel, a.best);
+                }
+                __syncthreads();                // the tile's words are all read
+                if (warp == 0) {
+                    // exclusive scan of the per-(item, warp) counts in
+                    // (item, warp) order
+                    constexpr int N = kRItems * kRWarps;
+                    constexpr int PER = N / 32;
+                    int cc[PER];
+                    int sum = 0;
+#pragma unroll
+                    for (int j = 0; j < PER; ++j) {
+                        const int idx = lane * PER + j;
+                        cc[j] = s_off[idx / kRWarps][idx % kRWarps];
+                        sum += cc[j];
+                    }
+                    int incl = sum;
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const int o = __shfl_up_sync(0xffffffffu, incl, d);
+                        if (lane >= d) incl += o;
+                    }
+                    int r = incl - sum;
+#pragma unroll
+                    for (int j = 0; j < PER; ++j) {
+                        const int idx = lane * PER + j;
+                        s_off[idx / kRWarps][idx % kRWarps] = r;
+                        r += cc[j];
+                    }
+                    if (lane == 31) s_base = incl;
+                }
+                __syncthreads();
+                const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+                for (int it = 0; it < kRItems; ++it)
+                    if (keep[it]) seg[out + s_off[it][warp] + __popc(bal[it] & lt)] = k[it];
+                out += s_base;
+                __syncthreads();                // s_off and s_base are reused
+            }
+            if (tid == 0) a.seg[q] = out;
+        }
+        if (!sync()) break;
+
+        // ---- E: the next round's sizes, the same in every participant ----
+        int64_t En = 0, An = 0;
+        {
+            int64_t x = 0, y = 0;
+            for (int64_t j = tid; j < Pe; j += kRT) {
+                x += __ldcg(a.seg + j);
+                y += __ldcg(a.alen + j);
+            }
+            block_excl_sum_shfl<kRT>(x, En);
+            block_excl_sum_shfl<kRT>(y, An);
+        }
+        if (tid == 0) s_err = *(volatile int *)a.err;
+        __syncthreads();
+        if (p == 0 && tid == 0 && round < kMaxRounds) {
+            a.trace[3 * round] = V;
+            a.trace[3 * round + 1] = E;
+            a.trace[3 * round + 2] = Aact;
+        }
+        ++round;
+        nmst += MODE == SEL_MST ? merges : 0;
+        if (s_err) done = 4;
+        else if (En == 0) done = 1;
+        else if (merges == 0) done = 2;
+        else if (round >= a.max_rounds) done = 3;
+        V -= merges;
+        E = En;
+        Aact = An;
+        __syncthreads();                        // s_err is rewritten next round
+        if (!done && !solo && An <= kSoloActive && En <= kSoloEdges) {
+            // every block decides alike: the others leave, and block 0 moves
+            // all active roots and edge words to the front of its own chunk
+            // and segment, in participant order (list order = id order is
+            // kept).  A destination never passes its source, so tiles are
+            // copied forward, each read before it is written.
+            solo = true;
+            if (p != 0) return;
+            int64_t ao = 0, eo = 0;
+            for (int64_t q = 0; q < Pe; ++q) {
+                const int64_t n = __ldcg(a.alen + q), m = __ldcg(a.seg + q);
+                const int32_t *asrc = a.act + vbase(q);
+                const uint64_t *esrc = a.e + ebase(q);
+                for (int64_t j = 0; j < n; j += kRT) {
+                    const int32_t v = j + tid < n ? __ldcg(asrc + j + tid) : 0;
+                    __syncthreads();
+                    if (j + tid < n) a.act[ao + j + tid] = v;
+                    __syncthreads();
+                }
+                for (int64_t j = 0; j < m; j += kRT) {
+                    const uint64_t v = j + tid < m ? __ldcg(esrc + j + tid) : 0ull;
+                    __syncthreads();
+                    if (j + tid < m) a.e[eo + j + tid] = v;
+                    __syncthreads();
+                }
+                ao += n;
+                eo += m;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                a.alen[0] = (int32_t)ao;
+                a.seg[0] = eo;
+            }
+            Pe = 1;
+            __syncthreads();
+        }
+    }
+    if (p == 0 && tid == 0) {
+        a.cnt[C_V] = V;
+        a.cnt[C_E] = E;
+        a.cnt[C_NMST] = nmst;
+        a.cnt[C_ROUNDS] = round;
+        a.cnt[C_ROUNDS_ALL] += round;
+        a.cnt[C_DONE] = done;
+        if (done == 2 || done == 3) set_err(a.err, DEV_CHASE_LIMIT);
+    }
+}
+
+// Points every original vertex at its root (the next phase's builds and the
+// final labels read roots directly).
+__global__ void k_flatten(int32_t *parent, int64_t V0, int *err)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x * 4;
+    for (int64_t xb = (int64_t)blockIdx.x * blockDim.x * 4 + threadIdx.x; xb < V0; xb += stride) {
+        int32_t x[4], r[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int64_t v = xb + (int64_t)i * blockDim.x;
+            x[i] = v < V0 ? (int32_t)v : -1;
+            r[i] = x[i];
+        }
+        find_batch<4>(parent, r, err);
+        (void)x;
+    }
+}
+
+// Component numbers = rank of the root id among all roots: the reference's
+// numbering (its per-round renumbering keeps root order).  flag/pos: V0
+// int32 scratch; labels may alias parent.
+__global__ void k_root_flags(const int32_t *parent, int64_t V0, int32_t *flag)
+{
+    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < V0;
+         x += (int64_t)gridDim.x * blockDim.x)
+        flag[x] = parent[x] == (int32_t)x;
+}
+
+__global__ void k_rank_roots(const int32_t *parent, const int32_t *pos, int64_t V0,
+                             int32_t *labels)
+{
+    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < V0;
+         x += (int64_t)gridDim.x * blockDim.x)
+        labels[x] = pos[parent[x]];
+}
+
+// Round-kernel launch shape.  Test hooks: g_round_cap lowers the rounds a
+// phase may run (reaching it is an error, as for the built-in cap), and
+// g_round_team forces the number of participants (1 = one block).
+static int g_round_cap = 0;
+static int g_round_team = 0;
+
+template <int MODE>
+static int round_team_max(int *out)
+{
+    static int cached = 0;
+    if (!cached) {
+        int dev = 0, sms = 0, per_sm = 0;
+        EACB_CUDA(cudaGetDevice(&dev));
+        EACB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        EACB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rounds<MODE, true>,
+                                                                kRT, 0));
+        int m = sms * (per_sm > 2 ? 2 : per_sm);
+        cached = m < 1 ? 1 : (m > kMaxTeam ? kMaxTeam : m);
+    }
+    *out = cached;
+    return EACB_OK;
+}
+
+// Participants for a graph of V0 vertices and at most Emax edge words: one
+// per 4096 vertices or 16K edge words, up to the resident maximum.
+template <int MODE>
+static int round_team(int64_t V0, int64_t Emax, int *team)
+{
+    int mx = 1;
+    int s = round_team_max<MODE>(&mx);
+    if (s) return s;
+    const int64_t work = std::max((V0 + 4095) / 4096, (Emax + 16383) / 16384);
+    int t = g_round_team > 0 ? g_round_team : (int)std::min<int64_t>(work, mx);
+    *team = std::max(1, std::min(t, mx));
+    return EACB_OK;
 }
 
 // MST selection key -> index of its entry in row min(u,v) of a symmetric CSR
@@ -1104,19 +1647,23 @@ __global__ void k_key2eid(const uint64_t *keys, int64_t n_keys, const int32_t *f
 // ---------------------------------------------------------------------------
 struct Engine {
     int *err;
-    int64_t *cnt;             // round state, indexed by C_E_NEXT .. C_DONE
-    uint64_t *ea, *eb;
-    int32_t *label;
+    int64_t *cnt;             // round state (C_*)
+    uint64_t *ea;             // edge words: phase builds write them, the rounds compact them
+    int32_t *label;           // union-find parent; after each phase every vertex's root
     unsigned long long *best;
-    int32_t *succ, *color, *flag, *pos;
+    int32_t *color, *flag, *pos, *act;
     uint64_t *mst;
     unsigned long long *hist; // 256 weight buckets
     int *lohi;                // the device phase plan (k_phase_plan)
+    int32_t *giant;           // root whose rows a later phase skips (k_pick_giant)
+    int32_t *part;            // per-participant counts of the round kernel
+    int32_t *alen;            // per-participant active roots
+    int64_t *seg;             // per-participant surviving edge words
+    int64_t *trace;
+    GridBarrier *bar;
     ScanScratch scan;
     int32_t V0;
     int64_t Emax;
-    int64_t mst_base = 0;     // forest edges emitted by earlier phases
-    int max_rounds = kMaxRounds;   // lowered only by the round-trace debug entry point
 
     static Engine carve(Carver &c, int32_t V0, int64_t Emax)
     {
@@ -1125,35 +1672,37 @@ struct Engine {
         g.cnt = c.take<int64_t>(C_COUNT);
         g.hist = c.take<unsigned long long>(256);
         g.lohi = c.take<int>(2 * kPhaseSlots);
+        g.giant = c.take<int32_t>(1);
+        g.bar = c.take<GridBarrier>(1);
+        g.seg = c.take<int64_t>(kMaxTeam);
+        g.trace = c.take<int64_t>(3 * kMaxRounds);
+        g.part = c.take<int32_t>(2 * kMaxTeam);
+        g.alen = c.take<int32_t>(kMaxTeam);
         g.V0 = V0;
-        g.Emax = Emax;
-        // one edge array (contraction is in place); eb holds the two
-        // directions of a forest (at most 2 V0 words) for the final clustering
-        g.ea = c.take<uint64_t>(Emax > 0 ? Emax : 1);
-        g.eb = c.take<uint64_t>(2 * (size_t)V0);
+        // the edge words (compacted in place by the rounds); they also hold
+        // the two directions of a forest (at most 2 V0 words)
+        g.Emax = std::max<int64_t>(Emax, 2 * (int64_t)V0);
+        g.ea = c.take<uint64_t>(g.Emax);
         g.label = c.take<int32_t>(V0);
         g.best = c.take<unsigned long long>(V0);
-        g.succ = c.take<int32_t>(V0);
         g.color = c.take<int32_t>(V0);
         g.flag = c.take<int32_t>(V0);
         g.pos = c.take<int32_t>(V0);
+        g.act = c.take<int32_t>(V0);
         g.mst = c.take<uint64_t>(V0);
-        g.scan = ScanScratch::carve(c, Emax > V0 ? Emax : V0, g.err);
+        g.scan = ScanScratch::carve(c, g.Emax, g.err);
         return g;
     }
 
-    int read_counts(cudaStream_t st, int64_t h[3])
+    int read_counts(cudaStream_t st, int64_t h[C_COUNT])
     {
         int e = 0;
-        EACB_CUDA(cudaMemcpyAsync(h, cnt, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        EACB_CUDA(cudaMemcpyAsync(h, cnt, C_COUNT * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
         EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
         EACB_CUDA(cudaStreamSynchronize(st));
         return dev_err_to_status(e);
     }
 
-    // MST by weight phases (see k_phase_csr).  `hist` must hold the 256-bucket
-    // weight histogram; build(lo, hi) launches one phase's edge build into ea
-    // (slots reserved through cnt[C_CURSOR]) with its selection into best.
     int read_hist(cudaStream_t st, unsigned long long h[256])
     {
         EACB_CUDA(cudaMemcpyAsync(h, hist, 256 * sizeof(unsigned long long),
@@ -1162,41 +1711,100 @@ struct Engine {
         return EACB_OK;
     }
 
+    int reset(cudaStream_t st)
+    {
+        EACB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+        EACB_CUDA(cudaMemsetAsync(cnt, 0, C_COUNT * sizeof(int64_t), st));
+        EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V0, st));
+        k_iota2<<<grid_for(V0, 256), 256, 0, st>>>(label, color, V0);
+        EACB_CHECK_LAUNCH();
+        return EACB_OK;
+    }
+
+    // Runs the rounds of one phase: input edges in ea (cnt[C_E] of them),
+    // supervertices [0, cnt[C_V]) with their selection in best.  One launch;
+    // with profiling on it is timed, and its algorithmic bytes come from the
+    // per-round sizes the kernel records.
+    template <int MODE>
+    int rounds(Pack pk, cudaStream_t st)
+    {
+        int team = 1;
+        int s = round_team<MODE>(V0, Emax, &team);
+        if (s) return s;
+        RoundArgs a;
+        a.pk = pk;
+        a.V0 = V0;
+        a.e = ea;
+        a.parent = label;
+        a.best = best;
+        a.color = color;
+        a.act = act;
+        a.mst = mst;
+        a.part = part;
+        a.alen = alen;
+        a.seg = seg;
+        a.cnt = cnt;
+        a.trace = trace;
+        a.bar = bar;
+        a.err = err;
+        a.max_rounds = g_round_cap > 0 ? std::min(g_round_cap, kMaxRounds) : kMaxRounds;
+        EACB_CUDA(cudaMemsetAsync(bar, 0, sizeof(GridBarrier), st));
+        ProfScope ps(PROF_ROUNDS, st);
+        if (team == 1) {
+            k_rounds<MODE, false><<<1, kRT, 0, st>>>(a);
+            EACB_CHECK_LAUNCH();
+        } else {
+            void *args[] = {(void *)&a};
+            EACB_CUDA(cudaLaunchCooperativeKernel((const void *)k_rounds<MODE, true>, dim3(team),
+                                                  dim3(kRT), args, 0, st));
+            count_launch();
+        }
+        if (ps.on) {
+            // per round: each edge word read and (if it survives) written
+            // back, 8 B each, with its two endpoints' parents (8 B); per
+            // active root its list entry, selection slot, successor and
+            // parent (20 B)
+            int64_t h[C_COUNT], tr[3 * kMaxRounds];
+            EACB_CUDA(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
+            EACB_CUDA(cudaMemcpyAsync(tr, trace, sizeof(tr), cudaMemcpyDeviceToHost, st));
+            EACB_CUDA(cudaStreamSynchronize(st));
+            double bytes = 0.0;
+            const int64_t nr = std::min<int64_t>(h[C_ROUNDS], kMaxRounds);
+            for (int64_t r = 0; r < nr; ++r) {
+                const double En = r + 1 < nr ? (double)tr[3 * r + 4] : (double)h[C_E];
+                bytes += 16.0 * (double)tr[3 * r + 1] + 8.0 * En + 20.0 * (double)tr[3 * r + 2];
+            }
+            ps.done(bytes);
+        }
+        // every vertex to its root, for the next phase's builds and the labels
+        k_flatten<<<grid_for(V0, 256 * 4, 148 * 8), 256, 0, st>>>(label, V0, err);
+        EACB_CHECK_LAUNCH();
+        return EACB_OK;
+    }
+
+    // MST by weight phases (see k_phase_csr), all queued back to back with no
+    // host read in between: build(ph) appends a phase's edges to ea through
+    // cnt[C_CURSOR] with their selection in best; k_phase_begin turns the
+    // cursor into the round kernel's edge count.  One read at the end gives
+    // the forest size, the component count and any error.
     template <typename Build>
     int run_phased(Pack pk, const std::vector<Phase> &plan, Build build, cudaStream_t st,
                    int64_t *n_mst_out, int64_t *n_comp_out)
     {
-        if (prof().enabled == 0 && max_rounds >= kMaxRounds) {
-            int per_round = 0;
-            cudaGraphExec_t exec = round_graph<SEL_MST>(pk, &per_round);
-            if (exec) return run_phased_graph(plan, build, exec, per_round, st, n_mst_out,
-                                              n_comp_out);
-        }
-        int32_t V = V0;
-        mst_base = 0;
-        for (const Phase &ph : plan) {
-            EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V, st));
+        for (size_t q = 0; q < plan.size(); ++q) {
+            EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V0, st));
             EACB_CUDA(cudaMemsetAsync(&cnt[C_CURSOR], 0, sizeof(int64_t), st));
-            EACB_CUDA(cudaMemsetAsync(hist, 0, 256 * sizeof(unsigned long long), st));
-            int s = build(ph);
+            int s = build(plan[q]);
             if (s) return s;
-            int64_t Ep = 0;
-            int e = 0;
-            EACB_CUDA(cudaMemcpyAsync(&Ep, &cnt[C_CURSOR], sizeof(int64_t), cudaMemcpyDeviceToHost,
-                                      st));
-            EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
-            EACB_CUDA(cudaStreamSynchronize(st));
-            if (e) return dev_err_to_status(e);
-            if (Ep > Emax) return EACB_ERR_INTERNAL;
-            if (prof().enabled) prof().bytes[PROF_PHASE] += 8.0 * (double)Ep;   // words written
-            int64_t nm = 0, nc = 0;
-            if ((s = run<SEL_MST>(pk, Ep, V, st, &nm, &nc))) return s;
-            mst_base += nm;
-            V = (int32_t)nc;
-            if (V <= 1) break;
+            k_phase_begin<<<1, 32, 0, st>>>(cnt, V0, q == 0 ? 1 : 0);
+            EACB_CHECK_LAUNCH();
+            if ((s = rounds<SEL_MST>(pk, st))) return s;
         }
-        *n_mst_out = mst_base;
-        *n_comp_out = V;
+        int64_t h[C_COUNT];
+        int s = read_counts(st, h);
+        if (s) return s;
+        *n_mst_out = h[C_NMST];
+        *n_comp_out = plan.empty() ? V0 : h[C_V];
         return EACB_OK;
     }
 
@@ -1208,8 +1816,7 @@ struct Engine {
     int run_phased_retry(Pack pk, std::vector<Phase> plan, Build build, Split split,
                          cudaStream_t st, int64_t *n_mst_out, int64_t *n_comp_out)
     {
-        int32_t V = V0;
-        mst_base = 0;
+        int64_t V = V0, n_mst = 0;
         size_t q = 0;
         while (q < plan.size()) {
             const Phase ph = plan[q];
@@ -1240,55 +1847,14 @@ struct Engine {
             if (e) return dev_err_to_status(e);
             if (Ep > Emax) return EACB_ERR_INTERNAL;
             if (prof().enabled) prof().bytes[PROF_PHASE] += 8.0 * (double)Ep;   // words written
-            int64_t nm = 0, nc = 0;
-            if ((s = run<SEL_MST>(pk, Ep, V, st, &nm, &nc))) return s;
-            mst_base += nm;
-            V = (int32_t)nc;
+            int64_t nc = 0;
+            if ((s = run<SEL_MST>(pk, Ep, V, st, &n_mst, &nc))) return s;
+            V = nc;
             ++q;
             if (V <= 1) break;
         }
-        *n_mst_out = mst_base;
+        *n_mst_out = n_mst;
         *n_comp_out = V;
-        return EACB_OK;
-    }
-
-    // All phases queued back to back with no host read in between: a phase's
-    // edge count and supervertex count stay on the device (k_phase_begin),
-    // an empty phase runs one no-op round, and one read at the end gives the
-    // forest size, the component count and any error.
-    template <typename Build>
-    int run_phased_graph(const std::vector<Phase> &plan, Build build, cudaGraphExec_t exec,
-                         int per_round, cudaStream_t st, int64_t *n_mst_out, int64_t *n_comp_out)
-    {
-        for (size_t q = 0; q < plan.size(); ++q) {
-            EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V0, st));
-            EACB_CUDA(cudaMemsetAsync(&cnt[C_CURSOR], 0, sizeof(int64_t), st));
-            int s = build(plan[q]);
-            if (s) return s;
-            k_phase_begin<<<1, 32, 0, st>>>(cnt, V0, q == 0 ? 1 : 0);
-            EACB_CHECK_LAUNCH();
-            EACB_CUDA(cudaGraphLaunch(exec, st));
-        }
-        int64_t after[C_COUNT];
-        int e = 0;
-        EACB_CUDA(cudaMemcpyAsync(after, cnt, sizeof(after), cudaMemcpyDeviceToHost, st));
-        EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
-        EACB_CUDA(cudaStreamSynchronize(st));
-        count_launch((int)(after[C_ROUNDS_ALL] * per_round));
-        if (e) return dev_err_to_status(e);
-        mst_base = after[C_NMST];
-        *n_mst_out = after[C_NMST];
-        *n_comp_out = plan.empty() ? V0 : after[C_V];
-        return EACB_OK;
-    }
-
-    int reset(cudaStream_t st)
-    {
-        EACB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
-        EACB_CUDA(cudaMemsetAsync(cnt, 0, C_COUNT * sizeof(int64_t), st));
-        EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V0, st));
-        k_iota<<<grid_for(V0, 256), 256, 0, st>>>(label, V0);
-        EACB_CHECK_LAUNCH();
         return EACB_OK;
     }
 
@@ -1296,249 +1862,38 @@ struct Engine {
     int filter(const Src &src, int64_t n_in, uint64_t *out, cudaStream_t st)
     {
         if (n_in == 0) {
-            EACB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int64_t), st));
+            EACB_CUDA(cudaMemsetAsync(&cnt[C_AUX0], 0, sizeof(int64_t), st));
             return EACB_OK;
         }
         const int64_t ntiles = (n_in + kETile - 1) / kETile;
         EACB_CUDA(cudaMemsetAsync(scan.status, 0, sizeof(uint64_t) * ntiles, st));
         EACB_CUDA(cudaMemsetAsync(scan.counter, 0, sizeof(int), st));
         k_edge_tile<MODE, Src><<<(unsigned)ntiles, kET, 0, st>>>(
-            src, n_in, out, best, scan.status, scan.counter, cnt, err);
+            src, n_in, out, best, scan.status, scan.counter, &cnt[C_AUX0], err);
         EACB_CHECK_LAUNCH();
         return EACB_OK;
     }
 
-    int edge_grid() const
-    {
-        const int64_t t = (Emax + kETile - 1) / kETile;
-        return (int)(t < 148 * 8 ? (t > 0 ? t : 1) : 148 * 8);
-    }
-
-    // One Boruvka round with every size read on the device (cnt[C_V],
-    // cnt[C_E]); identical launch shapes every round, so the sequence can be
-    // captured once into a CUDA graph.  With use_handle the last kernel sets
-    // the graph's loop condition.  Returns the kernels it launches per round
-    // in *per_round.
+    // Rounds from E0 edge words in ea (selection already in best) over
+    // supervertices [0, V_start).  On return: label = component of every
+    // vertex, *n_comp_out = number of components, *n_mst_total = forest
+    // edges emitted since the engine's reset.
     template <int MODE>
-    int enqueue_round(Pack pk, cudaStream_t st, int use_handle, cudaGraphConditionalHandle h,
-                      bool timed_filter, int *per_round)
-    {
-        const unsigned gv = 296;
-        int launches = 0;
-        // look-back status words: scans over V0, the contraction over Emax
-        const int64_t vtiles = (V0 + kScanTile - 1) / kScanTile;
-        const int64_t etiles = (Emax + kETile - 1) / kETile;
-        k_select<MODE><<<gv, 256, 0, st>>>(best, succ, &cnt[C_V], label, pk);
-        EACB_CHECK_LAUNCH();
-        k_mirror<<<gv, 256, 0, st>>>(succ, color, MODE == SEL_MST ? flag : nullptr, &cnt[C_V],
-                                     scan.status, vtiles, scan.counter);
-        EACB_CHECK_LAUNCH();
-        launches += 2;
-        if (MODE == SEL_MST) {
-            int s = scan_launch_dev<int32_t, int32_t>(flag, pos, &cnt[C_V], V0, 0, &cnt[C_EMIT],
-                                                      scan, st, false);
-            if (s) return s;
-            launches += 1;
-        }
-        k_jump<<<gv, 256, 0, st>>>(color, &cnt[C_V], err, best, flag, pos,
-                                   MODE == SEL_MST ? mst : nullptr, &cnt[C_NMST], scan.status,
-                                   vtiles, scan.counter);
-        EACB_CHECK_LAUNCH();
-        int s = scan_launch_dev<int32_t, int32_t>(flag, pos, &cnt[C_V], V0, 0, &cnt[C_V_NEXT],
-                                                  scan, st, false);
-        if (s) return s;
-        k_relabel<<<grid_for(V0, 256), 256, 0, st>>>(label, color, pos, V0, best, &cnt[C_V_NEXT],
-                                                       scan.status, etiles > 0 ? etiles : 1,
-                                                       scan.counter, &cnt[C_E_NEXT]);
-        EACB_CHECK_LAUNCH();
-        launches += 3;
-        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-        if (timed_filter) {
-            cudaEventCreate(&ev0);
-            cudaEventCreate(&ev1);
-            cudaEventRecord(ev0, st);
-        }
-        SrcEdges se{ea, label, pk, (uint32_t)V0};
-        k_edge_tile<MODE, SrcEdges><<<edge_grid(), kET, 0, st>>>(
-            se, 0, ea, best, scan.status, scan.counter, &cnt[C_E_NEXT], err, &cnt[C_E]);
-        EACB_CHECK_LAUNCH();
-        if (timed_filter) {
-            cudaEventRecord(ev1, st);
-            timed_ev0 = ev0;
-            timed_ev1 = ev1;
-        }
-        k_round_end<<<1, 32, 0, st>>>(cnt, MODE == SEL_MST ? 1 : 0, max_rounds, err, h, use_handle);
-        EACB_CHECK_LAUNCH();
-        launches += 2;
-        if (per_round) *per_round = launches;
-        return EACB_OK;
-    }
-
-    cudaEvent_t timed_ev0 = nullptr, timed_ev1 = nullptr;
-
-    template <int MODE>
-    cudaGraphExec_t round_graph(Pack pk, int *per_round);
-
-    // Rounds; edges of round 0 are in `ea` (E0 of them) and `best` holds
-    // their selection; supervertex ids are [0, V_start) under `label`.  The
-    // rounds run inside one CUDA graph that loops on the device (conditional
-    // WHILE node) until the phase converges; with profiling on (per-launch
-    // CUDA events) or a round limit they are driven from the host instead.
-    // On return: label = component of every vertex, *n_comp = number of
-    // components, *n_mst = forest edges emitted by these rounds.
-    template <int MODE>
-    int run(Pack pk, int64_t E0, int32_t V_start, cudaStream_t st, int64_t *n_mst_out,
+    int run(Pack pk, int64_t E0, int64_t V_start, cudaStream_t st, int64_t *n_mst_total,
             int64_t *n_comp_out)
     {
-        if (E0 == 0) {                 // nothing to contract: components stay as they are
-            *n_mst_out = 0;
-            *n_comp_out = V_start;
-            return EACB_OK;
-        }
-        int64_t before[C_COUNT];
-        EACB_CUDA(cudaMemcpyAsync(before, cnt, sizeof(before), cudaMemcpyDeviceToHost, st));
-        k_round_begin<<<1, 32, 0, st>>>(cnt, V_start, E0);
+        k_set_sizes<<<1, 32, 0, st>>>(cnt, V_start, E0);
         EACB_CHECK_LAUNCH();
-        int per_round = 0;
-        const bool host_driven = prof().enabled != 0 || max_rounds < kMaxRounds;
-        cudaGraphExec_t exec = host_driven ? nullptr : round_graph<MODE>(pk, &per_round);
-        int64_t after[C_COUNT];
-        int e = 0;
-        if (exec) {
-            EACB_CUDA(cudaGraphLaunch(exec, st));
-            EACB_CUDA(cudaMemcpyAsync(after, cnt, sizeof(after), cudaMemcpyDeviceToHost, st));
-            EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
-            EACB_CUDA(cudaStreamSynchronize(st));
-            count_launch((int)(after[C_ROUNDS] * per_round));
-        } else {
-            for (int round = 0; round < max_rounds; ++round) {
-                const bool timed = prof().enabled != 0;
-                int64_t E_in = 0;
-                if (timed)
-                    EACB_CUDA(cudaMemcpyAsync(&E_in, &cnt[C_E], sizeof(int64_t),
-                                              cudaMemcpyDeviceToHost, st));
-                int s = enqueue_round<MODE>(pk, st, 0, 0, timed, &per_round);
-                if (s) return s;
-                EACB_CUDA(cudaMemcpyAsync(after, cnt, sizeof(after), cudaMemcpyDeviceToHost, st));
-                EACB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
-                EACB_CUDA(cudaStreamSynchronize(st));
-                if (timed) {
-                    // algorithmic HBM bytes of one contraction: every edge word
-                    // read once, every surviving edge word written once
-                    float ms = 0.f;
-                    cudaEventElapsedTime(&ms, timed_ev0, timed_ev1);
-                    prof().ms[PROF_EDGE_TILE] += ms;
-                    prof().bytes[PROF_EDGE_TILE] +=
-                        8.0 * (double)E_in + 8.0 * (double)after[C_E_NEXT];
-                    prof().count[PROF_EDGE_TILE] += 1;
-                    cudaEventDestroy(timed_ev0);
-                    cudaEventDestroy(timed_ev1);
-                }
-                if (e || after[C_DONE]) break;
-            }
-        }
-        if (e) return dev_err_to_status(e);
-        const int64_t done = after[C_DONE];
-        if (done == 2) return EACB_ERR_NOT_CONVERGED;                 // no progress
-        if (done == 0 || done == 3) {                                  // round cap
-            if (max_rounds >= kMaxRounds) return EACB_ERR_NOT_CONVERGED;
-        }
-        *n_mst_out = after[C_NMST] - before[C_NMST];
-        *n_comp_out = after[C_V];
+        int s = rounds<MODE>(pk, st);
+        if (s) return s;
+        int64_t h[C_COUNT];
+        if ((s = read_counts(st, h))) return s;
+        if (h[C_DONE] != 1) return EACB_ERR_NOT_CONVERGED;
+        *n_mst_total = h[C_NMST];
+        *n_comp_out = h[C_V];
         return EACB_OK;
     }
 };
-
-// Cache of instantiated round graphs, keyed by everything the captured
-// kernels see (workspace layout, sizes, mode, key packing, device).
-struct GraphKey {
-    const void *base;
-    int64_t V0, Emax;
-    int mode, vbits, dev, max_rounds;
-    bool operator==(const GraphKey &o) const
-    {
-        return base == o.base && V0 == o.V0 && Emax == o.Emax && mode == o.mode &&
-               vbits == o.vbits && dev == o.dev && max_rounds == o.max_rounds;
-    }
-};
-struct GraphEntry {
-    GraphKey key;
-    cudaGraphExec_t exec;
-    int per_round;
-};
-// One cache per host thread: an entry is only ever launched by the thread
-// that built it, so no other thread can destroy a graph in use.
-struct GraphCache {
-    std::vector<GraphEntry> v;
-    ~GraphCache()
-    {
-        for (auto &g : v) cudaGraphExecDestroy(g.exec);
-    }
-};
-static thread_local GraphCache t_graphs;
-
-// Builds (once per key) the graph: a conditional WHILE node whose body is
-// one round; the body's last kernel clears the condition when the phase has
-// converged.  Returns nullptr if this driver cannot build it (the host then
-// drives the rounds).
-template <int MODE>
-cudaGraphExec_t Engine::round_graph(Pack pk, int *per_round)
-{
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
-    GraphKey key{(const void *)err, V0, Emax, MODE, pk.vbits, dev, max_rounds};
-    for (auto &g : t_graphs.v)
-        if (g.key == key) {
-            *per_round = g.per_round;
-            return g.exec;
-        }
-    cudaStream_t cs = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    int pr = 0;
-    bool ok = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaGraphCreate(&graph, 0) == cudaSuccess;
-    cudaGraphConditionalHandle h = 0;
-    if (ok) ok = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) ==
-                 cudaSuccess;
-    cudaGraphNodeParams cp = {};
-    cudaGraphNode_t node = nullptr;
-    if (ok) {
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        ok = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
-    }
-    if (ok) {
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        ok = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
-                                           cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-        if (ok) {
-            const int s = enqueue_round<MODE>(pk, cs, 1, h, false, &pr);
-            count_launch(-pr);                // capturing launches nothing
-            cudaGraph_t out = nullptr;
-            ok = cudaStreamEndCapture(cs, &out) == cudaSuccess && s == EACB_OK;
-        }
-    }
-    if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
-    if (graph) cudaGraphDestroy(graph);
-    if (cs) cudaStreamDestroy(cs);
-    cudaGetLastError();                       // a failed build leaves no sticky error
-    if (!ok) {
-        if (exec) cudaGraphExecDestroy(exec);
-        return nullptr;
-    }
-    if (t_graphs.v.size() >= 16) {
-        cudaGraphExecDestroy(t_graphs.v.front().exec);
-        t_graphs.v.erase(t_graphs.v.begin());
-    }
-    t_graphs.v.push_back(GraphEntry{key, exec, pr});
-    *per_round = pr;
-    return exec;
-}
-
-static int g_debug_rounds = 0;   // 0 = off; else rounds to run (round-trace test entry)
 
 template <typename WT>
 static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wbits,
@@ -1553,11 +1908,10 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
     Engine g = Engine::carve(c, V, E);
     if (c.overflow) return EACB_ERR_WORKSPACE;
     if ((s = g.reset(st))) return s;
-    int64_t h[3];
+    int64_t h[C_COUNT];
     int64_t n_mst = 0, n_comp = 0;
-    if (g_debug_rounds > 0) g.max_rounds = g_debug_rounds;
     const unsigned gr = grid_for((int64_t)V * 32, 256);
-    if (mode == SEL_MST && g_debug_rounds == 0) {
+    if (mode == SEL_MST) {
         // weight phases over the bucket histogram of the entries
         EACB_CUDA(cudaMemsetAsync(g.hist, 0, 256 * sizeof(unsigned long long), st));
         if (E > 0) {
@@ -1571,16 +1925,23 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
         }
         // the phase plan stays on the device: the whole MST is queued without
         // a host read until its end
-        k_phase_plan<<<1, 32, 0, st>>>(g.hist, g.lohi);
+        k_phase_plan<<<1, 256, 0, st>>>(g.hist, g.lohi);
         EACB_CHECK_LAUNCH();
         std::vector<Phase> plan;
         for (int q = 0; q < kPhaseSlots; ++q) plan.push_back(Phase{0, 0, 0, V, q});
-        // a phase holds a subset of the E entries: the edge array always fits
+        // a phase holds a subset of the E entries: the edge array always fits.
+        // The first phase reads every row with identity labels; the later one
+        // skips the rows of the giant component the first phase built
         auto build = [&](const Phase &ph) -> int {
             if (E == 0) return EACB_OK;
+            if (ph.slot > 0) {
+                k_pick_giant<<<1, 1024, 0, st>>>(g.label, V, g.giant);
+                EACB_CHECK_LAUNCH();
+            }
             ProfScope ps(PROF_PHASE, st);
             k_phase_csr<WT><<<gr, kPhThreads, 0, st>>>(
-                first, deg, dest, weight, V, E, wbits, 0, 0, g.lohi, ph.slot, g.label, pk, g.ea,
+                first, deg, dest, weight, V, E, wbits, 0, 0, g.lohi, ph.slot, ph.slot == 0 ? 1 : 0,
+                ph.slot > 0 ? g.giant : nullptr, g.label, pk, g.ea,
                 (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best,
                 g.err);
             EACB_CHECK_LAUNCH();
@@ -1594,35 +1955,33 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
         if (E > 0) {
             // dead words everywhere first: entries outside every row, self loops
             EACB_CUDA(cudaMemsetAsync(g.ea, 0xff, sizeof(uint64_t) * E, st));
-            if (mode == SEL_MST)
-                k_edges_csr<SEL_MST, WT><<<gr, 256, 0, st>>>(first, deg, dest, weight, V, E, pk,
-                                                             g.ea, g.best, g.err);
-            else
-                k_edges_csr<SEL_CC, WT><<<gr, 256, 0, st>>>(first, deg, dest, weight, V, E, pk,
-                                                            g.ea, g.best, g.err);
+            k_edges_csr<SEL_CC, WT><<<gr, 256, 0, st>>>(first, deg, dest, weight, V, E, pk, g.ea,
+                                                        g.best, g.err);
             EACB_CHECK_LAUNCH();
         }
-        if ((s = g.read_counts(st, h))) return s;      // input validity before the rounds
-        if (mode == SEL_MST) s = g.run<SEL_MST>(pk, E, V, st, &n_mst, &n_comp);
-        else s = g.run<SEL_CC>(pk, E, V, st, &n_mst, &n_comp);
-        if (s) return s;
+        if ((s = g.run<SEL_CC>(pk, E, V, st, &n_mst, &n_comp))) return s;
     }
     if (mode == SEL_MST) {
         if (n_mst > 0) {
             k_key2eid<WT><<<grid_for(n_mst, 256), 256, 0, st>>>(g.mst, n_mst, first, deg, dest,
-                                                                      weight, pk, mst_out, g.err);
+                                                                  weight, pk, mst_out, g.err);
             EACB_CHECK_LAUNCH();
         }
         if ((s = g.read_counts(st, h))) return s;
         *host_n_mst = n_mst;
     } else {
-        EACB_CUDA(cudaMemcpyAsync(labels_out, g.label, sizeof(int32_t) * V,
-                                  cudaMemcpyDeviceToDevice, st));
+        // the reference's component numbers: ranks of the root ids
+        const unsigned gv = grid_for(V, 256);
+        k_root_flags<<<gv, 256, 0, st>>>(g.label, V, g.flag);
+        EACB_CHECK_LAUNCH();
+        if ((s = scan_launch<int32_t, int32_t>(g.flag, g.pos, V, 0, &g.cnt[C_AUX1], g.scan, st)))
+            return s;
+        k_rank_roots<<<gv, 256, 0, st>>>(g.label, g.pos, V, labels_out);
+        EACB_CHECK_LAUNCH();
+        if ((s = g.read_counts(st, h))) return s;
+        if (h[C_AUX1] != n_comp) return EACB_ERR_INTERNAL;
         *host_n_comp = n_comp;
     }
-    if (g_debug_rounds > 0 && labels_out && mode == SEL_MST)
-        EACB_CUDA(cudaMemcpyAsync(labels_out, g.label, sizeof(int32_t) * V,
-                                  cudaMemcpyDeviceToDevice, st));
     return EACB_OK;
 }
 
@@ -1767,9 +2126,13 @@ __global__ void k_canon(const int32_t *label, const int32_t *cmin, const int32_t
 
 using namespace eacb;
 
-// Test hook: the next graph calls stop after `rounds` Boruvka rounds (0 =
-// run to completion) so tests can compare per-round state.
-extern "C" void eacb_debug_set_rounds(int rounds) { g_debug_rounds = rounds; }
+// Test hooks of the Boruvka round kernel (see k_rounds): the rounds a phase
+// may run (0 = the built-in cap; reaching a lower cap is reported as
+// EACB_ERR_NOT_CONVERGED, like the built-in one) and its participants
+// (0 = automatic, 1 = one block, more = that many cooperative blocks, at
+// most the resident maximum).  Process-wide; set them only between calls.
+extern "C" void eacb_debug_set_round_cap(int rounds) { g_round_cap = rounds > 0 ? rounds : 0; }
+extern "C" void eacb_debug_set_round_team(int blocks) { g_round_team = blocks > 0 ? blocks : 0; }
 
 extern "C" size_t eacb_boruvka_workspace_size(int32_t n_vertices, int64_t n_edges)
 {
@@ -1993,19 +2356,15 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
         *host_n_fclusts = 1;
         return EACB_OK;
     }
-    // 3. components of the forest without the cut edges (the forest keys
-    //    move to ea: the second run reuses the engine's buffers)
-    EACB_CUDA(cudaMemcpyAsync(g.ea, g.mst, sizeof(uint64_t) * n_mst, cudaMemcpyDeviceToDevice, st));
+    // 3. components of the forest without the cut edges: both directions of
+    //    the kept forest keys go from mst into ea, then the rounds
     if ((s = g.reset(st))) return s;
-    // the forest edges (both directions) go from ea[0, n_mst) into eb
-    SrcForest sf{g.ea, n_mst, hp.wmax, pk};
-    if ((s = g.filter<SEL_CC>(sf, 2 * n_mst, g.eb, st))) return s;
-    int64_t h[3];
+    SrcForest sf{g.mst, n_mst, hp.wmax, pk};
+    if ((s = g.filter<SEL_CC>(sf, 2 * n_mst, g.ea, st))) return s;
+    int64_t h[C_COUNT];
     if ((s = g.read_counts(st, h))) return s;
-    // run() starts from ea: swap roles by copying (forest is small)
-    EACB_CUDA(cudaMemcpyAsync(g.ea, g.eb, sizeof(uint64_t) * h[0], cudaMemcpyDeviceToDevice, st));
     int64_t nm2 = 0, nc2 = 0;
-    if ((s = g.run<SEL_CC>(pk, h[0], n, st, &nm2, &nc2))) return s;
+    if ((s = g.run<SEL_CC>(pk, h[C_AUX0], n, st, &nm2, &nc2))) return s;
     // 4. number components by their smallest member
     EACB_CUDA(cudaMemsetAsync(cmin, 0x7f, sizeof(int32_t) * n, st));
     const unsigned gn = grid_for(n, 256);
@@ -2013,11 +2372,12 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
     EACB_CHECK_LAUNCH();
     k_first_flag<<<gn, 256, 0, st>>>(g.label, cmin, n, g.flag);
     EACB_CHECK_LAUNCH();
-    if ((s = scan_launch<int32_t, int32_t>(g.flag, g.pos, n, 0, &g.cnt[1], g.scan, st))) return s;
+    if ((s = scan_launch<int32_t, int32_t>(g.flag, g.pos, n, 0, &g.cnt[C_AUX1], g.scan, st)))
+        return s;
     k_canon<<<gn, 256, 0, st>>>(g.label, cmin, g.pos, n, labels);
     EACB_CHECK_LAUNCH();
     if ((s = g.read_counts(st, h))) return s;
-    *host_n_fclusts = h[1];
+    *host_n_fclusts = h[C_AUX1];
     *host_labels_valid = 1;
     return EACB_OK;
 }

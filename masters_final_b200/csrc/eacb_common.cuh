@@ -277,7 +277,7 @@ __device__ __forceinline__ int64_t lookback(uint64_t *status, int64_t tile, int6
 // they are launched on, with their algorithmic byte counts.
 // ---------------------------------------------------------------------------
 namespace eacb {
-enum ProfTag { PROF_EDGE_TILE = 0, PROF_SCAN = 1, PROF_COASSOC = 2, PROF_KMEANS = 3,
+enum ProfTag { PROF_ROUNDS = 0, PROF_SCAN = 1, PROF_COASSOC = 2, PROF_KMEANS = 3,
                PROF_PHASE = 4, PROF_NTAGS = 8 };
 struct Prof {
     int enabled;

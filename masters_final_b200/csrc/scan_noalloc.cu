@@ -14,10 +14,13 @@
 // address of that array is looked up once per device with
 // cudaGetSymbolAddress (a lookup, not an allocation), on the first call made
 // while that device is current; make that first call before any stream
-// capture.  The array is shared by every call: the parts a call needs are
-// cleared at the start of the call, and two calls that run on the GPU at the
-// same time (for instance on two streams) would race on it, so callers must
-// serialise them.
+// capture.  The address is kept for the life of the process, so a process
+// that resets a device (cudaDeviceReset) must not call this entry point on
+// that device afterwards.  The array is shared by every call: the parts a
+// call needs are cleared at the start of the call, and two calls that run on
+// the GPU at the same time (for instance on two streams) would race on it, so
+// callers must serialise them.  Each call waits for its scan to finish: it
+// copies the device status back to the host and synchronizes the stream.
 #include "eacb_common.cuh"
 #include "scan_impl.cuh"
 
@@ -72,7 +75,9 @@ extern "C" int eacb_scan_excl_i32_noalloc(const int32_t *in, int32_t *out, int64
     // the previous call's contents are still there: clear what starts at zero
     // (scan_launch clears the tile counter and the status words it uses)
     EACB_CUDA(cudaMemsetAsync(sc.err, 0, sizeof(int), st));
+    eacb::ProfScope ps(eacb::PROF_SCAN, st);
     s = eacb::scan_launch<int32_t, int32_t>(in, out, n, init, d_total, sc, st);
+    ps.done((double)n * 2.0 * sizeof(int32_t));
     if (s) return s;
     // report a device-side failure of this call (a look-back wait that gave
     // up) before returning: read the error word and wait for the scan

@@ -1,9 +1,8 @@
 """Generate the golden fixtures by running the reference itself.
 
-Run in a checkout where the reference sources are present
-(``EAC_REFERENCE_ROOT``, default the read-only reference mount):
+Run where the reference sources are present, naming their root:
 
-    python tests/golden/make_golden.py
+    EAC_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden.py
 
 Every fixture is produced by the reference's own functions (loaded by
 ``refload.py``) on seeded synthetic inputs from

@@ -28,7 +28,18 @@ os.environ.setdefault("NUMBA_ENABLE_CUDASIM", "1")  # K_Means creates CUDA event
 
 import numpy as np
 
-REF = os.environ.get("EAC_REFERENCE_ROOT", "/root/reference")
+
+def _reference_root():
+    """The reference checkout, named by the EAC_REFERENCE_ROOT variable (no
+    default: the fixtures are only regenerated where the reference is)."""
+    root = os.environ.get("EAC_REFERENCE_ROOT")
+    if not root:
+        raise RuntimeError("set EAC_REFERENCE_ROOT to the reference checkout "
+                           "(the directory holding MyML/ and scipy_numba/)")
+    return root
+
+
+REF = _reference_root()
 
 _REWRITES = {
     "MyML/MyML/EAC/sparse.py": [

@@ -110,28 +110,39 @@ def test_boruvka_knn_1m_properties(T):
     _check_mst(indptr, dest, w, mst, n)
 
 
-def test_rounds_graph_vs_host_driven(T):
-    """The rounds run as one device-looping CUDA graph by default and from
-    the host with profiling on; both give the same forest and components,
-    and repeated calls reuse the cached graph."""
+@pytest.mark.parametrize("n,k,seed", [(200_000, 8, 11), (3000, 4, 12)])
+def test_round_team_sizes_agree(T, n, k, seed):
+    """The round kernel runs as one block or as a cooperative grid of any
+    size; the forest (as a set and in its emitted order) and the component
+    labels do not depend on it, and profiling (which times each launch and
+    reads the round sizes back) changes nothing."""
     from masters_final_b200 import _lib, workloads as W
     from masters_final_b200.graph.mst import boruvka_minho_gpu
     from masters_final_b200.graph.connected_components import connected_comps_gpu
-    indptr, dest, w = W.knn_graph(200_000, k=8, seed=11)
+    indptr, dest, w = W.knn_graph(n, k=k, seed=seed)
     first, deg = indptr[:-1].astype(np.int32), np.diff(indptr).astype(np.int32)
+    L = _lib.load()
     runs = []
-    for prof in (False, True, False):
-        _lib.profile_enable(prof)
-        try:
-            mst, n = boruvka_minho_gpu(dest, w, first, deg)
+    try:
+        for team, prof in ((0, False), (1, False), (2, False), (7, True), (1000, False)):
+            L.eacb_debug_set_round_team(team)
+            _lib.profile_enable(prof)
+            mst, nm = boruvka_minho_gpu(dest, w, first, deg)
             cc = connected_comps_gpu(dest, w, first, deg)
-        finally:
+            if prof:
+                _, ms, _, cnt = _lib.profile_read()
+                assert cnt[0] > 0 and ms[0] > 0          # round kernels were timed
             _lib.profile_enable(False)
-        runs.append((np.sort(mst[:n]), cc))
+            runs.append((mst[:nm].copy(), cc))
+    finally:
+        L.eacb_debug_set_round_team(0)
+        _lib.profile_enable(False)
     for mst, cc in runs[1:]:
         assert np.array_equal(mst, runs[0][0])
         assert np.array_equal(cc, runs[0][1])
     _check_mst(indptr, dest, w, runs[0][0], runs[0][0].size)
+    _, ref = oracle.boruvka_seq(indptr, dest, w)
+    assert np.array_equal(runs[0][1], ref)
 
 
 @pytest.mark.parametrize("dt", [np.uint16, np.int32, np.float32])
