@@ -45,6 +45,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-eac", action="store_true",
                     help="skip the EAC end-to-end measurements added to the line")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="skip the connected-components and scan measurements added to the line")
+    ap.add_argument("--case", choices=sorted(CASES),
+                    help="run one small named workload and exit (the cases the ncu summaries "
+                         "under profiles/ were captured on)")
     return ap.parse_args()
 
 
@@ -353,6 +358,11 @@ def run_ours(args):
     sharded = None
     if world > 1 and not args.no_eac:
         sharded = eac_batched_sharded_measurement(torch, dist, world)
+    graph = None
+    if world == 1 and not args.no_graph:
+        graph = {"cc_knn16_1M": cc_measurement(torch, (indptr, dest, w, d_dest, d_w, d_first,
+                                                         d_deg, ws), flush, args.steps),
+                 "scan_64m": scan_measurement(torch, flush, measured_peak()[0], args.steps)}
 
     if rank == 0:
         peak, peak_kind = measured_peak()
@@ -380,6 +390,8 @@ def run_ours(args):
                 "clocks": clk.summary()}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(indptr, dest, w, n_edges)
+        if graph is not None:
+            line["graph"] = graph
         if world == 1 and not args.no_eac:
             line["eac"] = eac_measurements(args)
         if sharded is not None:
@@ -388,6 +400,118 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------ graph --
+def _timed(torch, fn, steps, warm, flush):
+    """Median CUDA-event milliseconds of fn() on the current stream, L2 flushed
+    (a 256 MiB write) before each timed call."""
+    st = torch.cuda.current_stream()
+    for _ in range(warm):
+        fn()
+    ms = []
+    for i in range(steps):
+        flush.fill_(i & 255)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        fn()
+        b.record(st)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    return statistics.median(ms)
+
+
+def cc_measurement(torch, graph, flush, steps):
+    """Connected components of the 16-NN graph (the reference's numbering):
+    undirected edges/s device-resident, and end to end through
+    connected_comps_gpu with pinned host buffers; CPU: the oracle's C
+    restatement of the reference's Boruvka rounds, which connected_comps_seq
+    runs with its labels tracked (one core)."""
+    import ctypes
+    import oracle
+    from masters_final_b200 import _lib
+    from masters_final_b200.graph.connected_components import connected_comps_gpu
+    indptr, dest, w, d_dest, d_w, d_first, d_deg, ws = graph
+    L = _lib.load()
+    V, E = indptr.size - 1, dest.size
+    n_edges = E // 2
+    labels = torch.empty(V, dtype=torch.int32, device="cuda")
+    nc = ctypes.c_int64(0)
+    sh = _lib.stream_handle()
+
+    def step():
+        _lib.check(L.eacb_connected_components(_lib.ptr(d_dest), _lib.ptr(d_w), _lib.U8,
+                                               _lib.ptr(d_first), _lib.ptr(d_deg), V, E,
+                                               _lib.ptr(labels), ctypes.byref(nc), _lib.ptr(ws),
+                                               ws.numel(), sh), "connected components")
+    ms = _timed(torch, step, steps, 3, flush)
+    h = [torch.from_numpy(a).pin_memory() for a in
+         (dest, w, indptr[:-1].astype(np.int32), np.diff(indptr).astype(np.int32))]
+    e_ms = _timed(torch, lambda: connected_comps_gpu(*h), max(3, steps // 2), 2, flush)
+    # cpu_baseline leg: the oracle, timed
+    t0 = time.perf_counter()
+    oracle.boruvka_seq(indptr, dest, w)
+    cpu_s = time.perf_counter() - t0
+    return {"metric": "CC edges/s", "value": n_edges / (ms / 1e3), "unit": "edges/s",
+            "ms": ms, "n_components": int(nc.value),
+            "e2e": {"value": n_edges / (e_ms / 1e3), "unit": "edges/s", "ms": e_ms,
+                    "h2d_bytes_per_step": int(sum(x.numel() * x.element_size() for x in h)),
+                    "d2h_bytes_per_step": int(4 * V)},
+            "cpu_baseline": {"value": n_edges / cpu_s, "unit": "edges/s", "cores": 1,
+                             "kind": "port", "sample": "full graph, one run of the oracle's C "
+                             "restatement of the reference's Boruvka rounds (the rounds "
+                             "connected_comps_seq runs, labels tracked)"},
+            "config": {"workload": "cc_knn16_1M", "graph": "the MST workload's graph"}}
+
+
+def scan_measurement(torch, flush, peak, steps):
+    """Exclusive scan of 64 Mi int32 uniform in [0, 1000]: int32 (wrapping,
+    8 B per element) and int32 -> int64 (12 B per element) outputs; GB/s
+    and fraction of the measured HBM copy bandwidth; end to end through
+    exprefixsumNumba with pinned host arrays; CPU: the oracle's restatement
+    of exprefixsumNumba (one core)."""
+    import ctypes
+    import oracle
+    from masters_final_b200 import _lib, workloads as W
+    from masters_final_b200.utils.scan import exprefixsumNumba
+    L = _lib.load()
+    n = 64 << 20
+    a = W.scan_input(n, seed=3)
+    total = int(a.astype(np.int64).sum())
+    x = torch.from_numpy(a).cuda()
+    tot = torch.empty(1, dtype=torch.int64, device="cuda")
+    ws = torch.empty(L.eacb_scan_workspace_size(n), dtype=torch.uint8, device="cuda")
+    sh = _lib.stream_handle()
+    out = {}
+    for name, fn, odt, bpe in (("i32", L.eacb_scan_excl_i32, torch.int32, 8),
+                               ("i32_i64", L.eacb_scan_excl_i32_i64, torch.int64, 12)):
+        o = torch.empty(n, dtype=odt, device="cuda")
+
+        def step():
+            _lib.check(fn(_lib.ptr(x), _lib.ptr(o), n, 0, _lib.ptr(tot), _lib.ptr(ws), ws.numel(),
+                          sh), "scan")
+        ms = _timed(torch, step, steps, 5, flush)
+        gbs = n * bpe / (ms / 1e3) / 1e9
+        out[name] = {"ms": ms, "gb_per_s": gbs, "bytes_per_element": bpe,
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak,
+                                  "unit": "GB/s", "frac": gbs / peak},
+                     "total_exact": int(tot.item()) == total}
+        del o
+    hin = torch.from_numpy(a).pin_memory()
+    hout = torch.empty(n, dtype=torch.int32).pin_memory()
+    e_ms = _timed(torch, lambda: exprefixsumNumba(hin, hout), 3, 1, flush)
+    out["e2e"] = {"value": n / (e_ms / 1e3), "unit": "elements/s", "ms": e_ms,
+                  "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * n,
+                  "differences_give_input": bool(np.array_equal(np.diff(hout.numpy()), a[:-1]))}
+    # cpu_baseline leg: the oracle, timed
+    t0 = time.perf_counter()
+    oracle.exprefixsum(a)
+    cs = time.perf_counter() - t0
+    out["cpu_baseline"] = {"value": n * 8 / cs / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
+                           "sample": "64 Mi int32, one run of the oracle's C restatement of "
+                                     "exprefixsumNumba"}
+    out["config"] = {"workload": "scan_64m", "n": n, "values": "int32 uniform [0, 1000]"}
+    return out
 
 
 # EAC end to end (ensemble -> co-association -> Boruvka MST -> lifetime cut)
@@ -409,7 +533,8 @@ EAC_BATCHED = dict(instances=512, P=50, seed=0, workers=32)
 
 
 def eac_run_once(X, cfg, mode, torch):
-    """One full EAC pipeline on device-resident data; per-stage CUDA events."""
+    """One full EAC pipeline on device-resident data; per-stage CUDA events.
+    Returns (stage ms, final labels, the EAC object, the label matrix)."""
     import random
     from masters_final_b200.utils.partition import generate_ensemble_labels
     from masters_final_b200.EAC.eac import EAC
@@ -426,17 +551,31 @@ def eac_run_once(X, cfg, mode, torch):
     ev[3].record()
     ev[3].synchronize()
     ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(3)]
-    return ms, labels, e
+    return ms, labels, e, L
+
+
+def pair_updates(torch, L):
+    """Co-association pair updates of a label matrix: sum over partitions and
+    clusters of |c| (|c| - 1) / 2 (the reference's inner-loop count)."""
+    tot = 0
+    for r in L:
+        c = torch.bincount(r[r >= 0]).to(torch.int64)
+        tot += int((c * (c - 1) // 2).sum().item())
+    return tot
 
 
 def eac_measurements(args):
     """EAC points/s of the BF16 tensor-core and the FP32 pipelines on the
-    10k-point (reference CPU-runnable) and 500k-point workloads; both
-    pipelines must produce identical final partitions."""
+    10k-, 500k- and 2M-point workloads (both pipelines must produce
+    identical final partitions), with the reference CPU path beside each
+    (the oracle's C restatement, one core: in full at 10k points,
+    extrapolated from measured per-stage rates at 500k and 2M); and the
+    512-dataset workload batched (BF16) and one dataset at a time (FP32)."""
     import torch
     from masters_final_b200 import workloads as W
     out = {}
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    rates = None
     for name, cfg in EAC_WORKLOADS.items():
         x = W.gaussian_mixture(cfg["n"], cfg["d"], cfg["comps"], seed=cfg["seed"],
                                sigma=cfg["sigma"], center_range=cfg["cr"],
@@ -447,22 +586,18 @@ def eac_measurements(args):
         res = {}
         parts = {}
         e = None
-        def release():
-            # large workloads: the previous matrix goes before the next one is
-            # built (small ones keep the allocator's cache, as a user would)
-            if not small:
-                torch.cuda.empty_cache()
+        L = None
+        # the warm-up run leaves the allocator's cache holding the arrays the
+        # timed runs reuse (the stage times are kernels, not cudaMalloc)
         for mode in ("bf16", "cuda"):
             for _ in range(warm):
-                e = None
-                release()
+                e = L = None
                 eac_run_once(X, cfg, mode, torch)
             tot = [0.0, 0.0, 0.0]
             for _ in range(steps):
-                e = None
-                release()
+                e = L = None
                 flush.fill_(1)
-                ms, labels, e = eac_run_once(X, cfg, mode, torch)
+                ms, labels, e, L = eac_run_once(X, cfg, mode, torch)
                 tot = [a + b for a, b in zip(tot, ms)]
             total_ms = sum(tot) / steps
             key = "bf16_tc" if mode == "bf16" else "fp32"
@@ -474,12 +609,121 @@ def eac_measurements(args):
         res["nnz"] = int(e.coassoc.nnz)
         res["nnz_discarded"] = int(e.coassoc.nnz_discarded)
         res["n_fclusts"] = int(e.n_fclusts)
+        pairs = pair_updates(torch, L)
+        res["pair_updates"] = pairs
+        res["pair_updates_per_s"] = pairs / (res["bf16_tc"]["ms_coassoc"] / 1e3)
         res["config"] = {k: (list(v) if isinstance(v, tuple) else v) for k, v in cfg.items()}
+        if not args.no_cpu_baseline:
+            if rates is None:
+                res["cpu_baseline"], rates = eac_cpu_full(x, cfg)
+            else:
+                res["cpu_baseline"] = eac_cpu_extrapolated(x, cfg, rates, pairs, res["nnz"])
         out[name] = res
-        del X, e
+        del X, e, L
         torch.cuda.empty_cache()
-    out["eac_batched_512"] = eac_batched_measurement(torch)
+    out["eac_batched_512"] = eac_batched_measurement(torch, args)
     return out
+
+
+# ------------------------------------------------ EAC reference CPU path --
+def _oracle_eac_timed(x, ks, inits, P):
+    """The reference EAC pipeline restated on the CPU (oracle, one core):
+    per-stage seconds and the work counts."""
+    import oracle
+    nc, _, nnz, _, secs, pairs = oracle.eac_pipeline(x, ks, inits, P)
+    return {"s": secs, "nnz": int(nnz), "pairs": pairs, "n_fclusts": int(nc)}
+
+
+def eac_cpu_full(x, cfg):
+    """The 10k-point workload through the oracle pipeline in full, with the
+    same draws as the GPU run; also returns the measured rates that the
+    larger workloads are extrapolated from."""
+    import random
+    from masters_final_b200.utils.partition import draw_ensemble_params
+    np.random.seed(cfg["seed"])
+    random.seed(cfg["seed"])
+    n = x.shape[0]
+    ks, inits = draw_ensemble_params(n, list(cfg["k"]), cfg["P"])
+    r = _oracle_eac_timed(x, ks, inits, cfg["P"])
+    tot = sum(r["s"])
+    rates = {"pairs_per_s": r["pairs"] / r["s"][1], "kruskal_entries_per_s": r["nnz"] / r["s"][2]}
+    return ({"value": n / tot, "unit": "points/s", "cores": 1, "kind": "port",
+             "sample": "the full workload, once: the oracle's C restatement of generateEnsemble "
+                       "+ K_Means.fit, EAC_CSR.update_ensemble and sp_sl_lifetime (Kruskal + "
+                       "lifetime cut), single-threaded like the reference",
+             "stage_s": r["s"], **rates}, rates)
+
+
+def eac_cpu_extrapolated(x, cfg, rates, pairs, nnz, n_sample=20_000):
+    """Reference CPU time of a workload too large to run on the host within
+    the bench: the ensemble timed on one partition pair over n_sample
+    points (linear in n at fixed k) scaled to n and P; the co-association
+    and the Kruskal stage from the pair-update and entry rates the 10k-point
+    run measured, applied to this workload's counts (from the GPU run).
+    Those rates come from rows of a few hundred entries; the reference's
+    sorted-row insertion costs more per pair on longer rows, so the
+    estimate is a lower bound of the CPU time."""
+    import oracle
+    import random
+    n = x.shape[0]
+    rng = np.random.default_rng(cfg["seed"] + 1)
+    xs = np.ascontiguousarray(x[rng.choice(n, n_sample, replace=False)])
+    np.random.seed(cfg["seed"])
+    random.seed(cfg["seed"])
+    ks = [int(np.random.randint(cfg["k"][0], cfg["k"][1])) for _ in range(2)]
+    inits = [random.sample(range(n_sample), k) for k in ks]
+    t0 = time.perf_counter()
+    oracle.ensemble_labels(xs, list(zip(ks, inits)))
+    t_ens = (time.perf_counter() - t0) / 2 * (n / n_sample) * cfg["P"]
+    t_co = pairs / rates["pairs_per_s"]
+    t_fin = nnz / rates["kruskal_entries_per_s"]
+    tot = t_ens + t_co + t_fin
+    return {"value": n / tot, "unit": "points/s", "cores": 1, "kind": "port",
+            "extrapolated": True,
+            "sample": "extrapolated: ensemble = 2 partitions on %d sampled points x (n / %d) x "
+                      "P; co-association = this workload's %d pair updates at the 10k-point "
+                      "run's measured rate; Kruskal = its %d entries at that run's rate"
+                      % (n_sample, n_sample, pairs, nnz),
+            "stage_s": [t_ens, t_co, t_fin]}
+
+
+def eac_batched_cpu(xs, ps, P):
+    """The 512-dataset workload on the host: a cost-spread sample of
+    datasets through the oracle pipeline on one core, and as many datasets
+    as host threads through a spawned process pool (one per thread); both
+    scaled to all datasets by the instances' relative costs."""
+    import multiprocessing as mp
+    from masters_final_b200.EAC.batched import instance_cost
+    cost = np.array([instance_cost(x.shape[0], x.shape[1], P, max(k))
+                     for x, (k, _) in zip(xs, ps)])
+    order = np.argsort(cost)
+    N = float(sum(x.shape[0] for x in xs))
+    # samples from the lower two-thirds of the cost range keep this leg to
+    # tens of seconds; the scaling by relative cost covers the rest
+    hi = max(1, int(0.65 * (len(xs) - 1)))
+    one = order[np.linspace(int(0.2 * hi), hi, 4).round().astype(int)]
+    import oracle
+    t1 = sum(oracle.eac_pipeline_seconds((xs[i], ps[i][0], ps[i][1], P)) for i in one)
+    est1 = t1 * cost.sum() / cost[one].sum()
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    cores = max(1, min(cores or 1, 64))
+    many = order[np.linspace(int(0.15 * hi), hi, cores).round().astype(int)]
+    with mp.get_context("spawn").Pool(cores) as pool:
+        pool.map(oracle.eac_pipeline_seconds,
+                 [(xs[one[0]], ps[one[0]][0], ps[one[0]][1], P)] * cores)
+        t0 = time.perf_counter()
+        pool.map(oracle.eac_pipeline_seconds, [(xs[i], ps[i][0], ps[i][1], P) for i in many],
+                 chunksize=1)
+        tw = time.perf_counter() - t0
+    estn = tw * cost.sum() / cost[many].sum()
+    return {"value": N / est1, "unit": "points/s", "cores": 1, "kind": "port",
+            "extrapolated": True,
+            "sample": "4 datasets from the lower two-thirds of the cost range through the oracle "
+                      "pipeline on one core (%.1f s), scaled to all %d by relative cost "
+                      "(EAC.batched.instance_cost)" % (t1, len(xs)),
+            "host": {"value": N / estn, "unit": "points/s", "cores": cores,
+                     "sample": "%d datasets on %d spawned processes at once (%.1f s wall), "
+                               "scaled to all %d by relative cost" % (cores, cores, tw, len(xs))}}
 
 
 def eac_batched_sharded_measurement(torch, dist, world):
@@ -507,11 +751,16 @@ def eac_batched_sharded_measurement(torch, dist, world):
             "config": {**cfg, "label_mode": "bf16"}}
 
 
-def eac_batched_measurement(torch):
+def eac_batched_measurement(torch, args):
     """Batched EAC points/s (sum of n over all datasets / wall time of one
-    eac_batch call, data on the device), after one warm-up call."""
+    eac_batch call, BF16 labels, data on the device), after one warm-up
+    call; beside it the same datasets run one at a time through the
+    single-instance pipeline with the FP32 labeler, whose final partitions
+    must be identical; and the reference CPU path."""
+    import random
     from masters_final_b200 import workloads as W
     from masters_final_b200.EAC.batched import eac_batch, draw_instance_params, k_range_rule1
+    from masters_final_b200.EAC.eac import eac_pipeline
     cfg = EAC_BATCHED
     xs = W.batched_instances(cfg["instances"], seed=cfg["seed"])
     ps = [draw_instance_params(x.shape[0], k_range_rule1(x.shape[0]), cfg["P"], i)
@@ -525,18 +774,127 @@ def eac_batched_measurement(torch):
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     st = np.array([a.ms_stages for a in r])
-    return {"points_per_s": N / dt, "s": dt, "sum_n": N, "instances": len(xs),
-            "nnz_total": int(sum(a.nnz for a in r)),
-            "nnz_discarded_total": int(sum(a.nnz_discarded for a in r)),
-            "failed": int(sum(a.status != 0 for a in r)),
-            "worker_ms_sums": {"ensemble": float(st[:, 0].sum()), "coassoc": float(st[:, 1].sum()),
-                               "final": float(st[:, 2].sum())},
-            "config": {**cfg, "n_range": [1000, 50000], "d": [2, 4, 8, 16, 32],
-                       "gaussians": [3, 30], "sigma": [0.5, 2.0], "label_mode": "bf16"}}
+    out = {"points_per_s": N / dt, "s": dt, "sum_n": N, "instances": len(xs),
+           "nnz_total": int(sum(a.nnz for a in r)),
+           "nnz_discarded_total": int(sum(a.nnz_discarded for a in r)),
+           "failed": int(sum(a.status != 0 for a in r)),
+           "worker_ms_sums": {"ensemble": float(st[:, 0].sum()), "coassoc": float(st[:, 1].sum()),
+                              "final": float(st[:, 2].sum())},
+           "config": {**cfg, "n_range": [1000, 50000], "d": [2, 4, 8, 16, 32],
+                      "gaussians": [3, 30], "sigma": [0.5, 2.0], "label_mode": "bf16"}}
+    # the plain single-instance pipeline: FP32 labeler, one dataset at a time
+    def single(i):
+        np.random.seed(i)
+        random.seed(i)
+        return eac_pipeline(Xd[i], cfg["P"], k_range_rule1(xs[i].shape[0]), label_mode="cuda")
+    single(0)
+    torch.cuda.synchronize()
+    same = True
+    t0 = time.perf_counter()
+    for i in range(len(xs)):
+        nf, lab, _ = single(i)
+        rb = r[i]
+        if rb.labels_valid:
+            same = same and nf == rb.n_fclusts and np.array_equal(lab, rb.labels.cpu().numpy())
+        else:
+            same = same and nf <= 1
+    torch.cuda.synchronize()
+    ds = time.perf_counter() - t0
+    out["single_instance_fp32"] = {"points_per_s": N / ds, "s": ds, "identical_partitions": same,
+                                   "timing": "host wall clock around 512 sequential "
+                                             "eac_pipeline calls (label_mode cuda)"}
+    out["batched_over_single_fp32"] = (N / dt) / (N / ds)
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = eac_batched_cpu(xs, ps, cfg["P"])
+    return out
+
+
+# ------------------------------------------------- profiling cases --------
+def case_label_tc_100k():
+    """K-Means ensemble on the tensor-core labeler: 100,000 16-D points from
+    50 anisotropic Gaussians (the 500k workload's mixture), 2 partitions, k
+    in [350, 711), 3 Lloyd iterations."""
+    import torch
+    from masters_final_b200 import workloads as W
+    from masters_final_b200.cluster.KMeans import kmeans_ensemble
+    x = W.gaussian_mixture(100_000, 16, 50, seed=3, center_range=20.0, anisotropic=True)
+    rng = np.random.default_rng(4)
+    ks = [int(k) for k in rng.integers(350, 711, 2)]
+    inits = [rng.choice(x.shape[0], k, replace=False).tolist() for k in ks]
+    X = torch.from_numpy(x).cuda()
+    for _ in range(2):
+        out = kmeans_ensemble(X, ks, inits, max_iter=3, label_mode="bf16")
+    torch.cuda.synchronize()
+    return {"ks": ks, "iters": out[3].tolist()}
+
+
+def case_mst_knn16_1M():
+    """Three Boruvka MST calls on the 16-NN graph of 1,000,000 points."""
+    import torch
+    from masters_final_b200 import workloads as W
+    from masters_final_b200.graph.mst import boruvka_minho_gpu
+    indptr, dest, w = W.knn_graph(N_VERTICES, k=KNN, seed=SEED)
+    d = [torch.from_numpy(a).cuda() for a in (dest, w, indptr[:-1].astype(np.int32),
+                                               np.diff(indptr).astype(np.int32))]
+    for _ in range(3):
+        _, n = boruvka_minho_gpu(*d, returnDevAry=True)
+    torch.cuda.synchronize()
+    return {"n_mst": n}
+
+
+def case_coassoc300k():
+    """Co-association count and fill of 300,000 16-D points from 50
+    anisotropic Gaussians (centres in [-20, 20]^16), 100 K-Means partitions
+    with k in [210, 427) (BF16 labels), linear capacity, factor 3."""
+    import random
+    import torch
+    from masters_final_b200 import workloads as W
+    from masters_final_b200.EAC.sparse import CoassocBuilder, EAC_CSR
+    from masters_final_b200.utils.partition import generate_ensemble_labels
+    x = W.gaussian_mixture(300_000, 16, 50, seed=3, center_range=20.0, anisotropic=True)
+    np.random.seed(3)
+    random.seed(3)
+    L, _ = generate_ensemble_labels(torch.from_numpy(x).cuda(), [210, 427], 100, 3,
+                                    label_mode="bf16")
+    b = CoassocBuilder(L, x.shape[0])
+    c = EAC_CSR(x.shape[0], max_assocs=int(b.max_cluster * 3), condensed=True,
+                max_assocs_type="linear")
+    c.update_ensemble(None, builder=b)
+    torch.cuda.synchronize()
+    return {"nnz": int(c.nnz)}
+
+
+def case_final_phase_synthetic():
+    """EAC final clustering of a synthetic condensed matrix: 100,000 rows,
+    row i holding min(5000, n-1-i) columns spread over (i, n), uint8 weights
+    101 - floor(100 u^0.25), max_dist 100."""
+    import torch
+    from masters_final_b200.EAC.eac import sp_sl_lifetime_csr
+    n, m = 100_000, 5000
+    rng = np.random.default_rng(6)
+    deg = np.minimum(m, n - 1 - np.arange(n)).astype(np.int64)
+    indptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(deg, out=indptr[1:])
+    rows = np.repeat(np.arange(n), deg)
+    span = (n - 1 - rows).astype(np.float64)
+    pos = np.arange(indptr[-1]) - indptr[rows]
+    cols = (rows + 1 + np.floor(pos * span / np.maximum(deg[rows], 1))).astype(np.int32)
+    w = (101 - np.floor(100 * rng.random(pos.size) ** 0.25)).astype(np.uint8)
+    d = [torch.from_numpy(a).cuda() for a in (indptr, cols, w)]
+    nc, _ = sp_sl_lifetime_csr(d[0], d[1], d[2], n, 100, returnDevAry=True)
+    torch.cuda.synchronize()
+    return {"entries": int(indptr[-1]), "n_fclusts": int(nc)}
+
+
+CASES = {"label_tc_100k": case_label_tc_100k, "mst_knn16_1M": case_mst_knn16_1M,
+         "coassoc300k": case_coassoc300k, "final_phase_synthetic": case_final_phase_synthetic}
 
 
 def main():
     args = parse()
+    if args.case:
+        print(json.dumps({"case": args.case, **CASES[args.case]()}), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

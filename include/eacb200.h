@@ -78,6 +78,24 @@ int eacb_workspace_status(void *ws, uintptr_t stream);
 void eacb_profile_enable(int on);
 void eacb_profile_read(int64_t *launches, double *ms, double *bytes, int64_t *count);
 
+/* Launch-shape tuning table (no counterpart in the reference, which has
+ * fixed launch shapes: MyML/MyML/cluster/KMeans.py:286-291).  Knobs, each
+ * with a built-in default and a shape (a, b): 0 tensor-core labeler CTAs
+ * per SM (1 or 2; a = d, b = n), 1 its centroid tile buffers (1 or 2),
+ * 2 co-association count pass CTAs per SM (a = P, b = n), 3 fill pass CTAs
+ * per SM, 4 the graph MST's first weight phase as a share of the entries
+ * in per mille (a = 0, b = vertices), 5 the Boruvka round kernel's
+ * participants at most (a = 0 graph MST/CC, 1 EAC final clustering;
+ * b = vertices).  eacb_tune_set adds an entry for a <= .. <= a_hi and
+ * b_lo <= .. <= b_hi (the first matching entry wins); eacb_tune_clear
+ * removes all; eacb_tune_get returns the value a launch of shape (a, b)
+ * would use (dflt when no entry matches).  Process-wide; set it between
+ * calls (the Python binding loads masters_final_b200/tuning.json at start). */
+int eacb_tune_set(int knob, int64_t a_lo, int64_t a_hi, int64_t b_lo, int64_t b_hi,
+                  int64_t value);
+void eacb_tune_clear(void);
+int64_t eacb_tune_get(int knob, int64_t a, int64_t b, int64_t dflt);
+
 /* Test hooks of the Boruvka round kernel, process-wide, to be set between
  * calls.  eacb_debug_set_round_cap: rounds a weight phase may run (0 = the
  * built-in cap of 96); a graph that needs more returns

@@ -52,7 +52,7 @@ def draw_instance_params(n, k_range, n_partitions, seed):
 
 def eac_batch(datasets, n_partitions=50, k_ranges=None, seeds=None, iters=3, tol=1e-4,
               label_mode="bf16", centroid_mode="numba", max_assocs_factor=3,
-              max_assocs_type="linear", n_clusters=0, n_workers=16, arena_bytes=None,
+              max_assocs_type="linear", n_clusters=0, n_workers=None, arena_bytes=None,
               params=None, return_device=False, stream=None):
     """Run EAC on every dataset of ``datasets`` (list of (n_i, d_i) float32
     arrays, numpy or CUDA tensors; d_i <= 32).
@@ -71,6 +71,8 @@ def eac_batch(datasets, n_partitions=50, k_ranges=None, seeds=None, iters=3, tol
     m = len(datasets)
     if m == 0:
         return []
+    if n_workers is None:
+        n_workers = int(_lib.tuned("batched_workers", 16))
     if max_assocs_type not in ("linear", "constant"):
         raise ValueError("max_assocs_type must be 'linear' or 'constant'")
     if n_clusters < 0:

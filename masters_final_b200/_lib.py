@@ -58,6 +58,9 @@ def load():
         "eacb_scan_excl_i32": (ctypes.c_int, [p, p, i64, i64, p, p, sz, p]),
         "eacb_scan_excl_i32_i64": (ctypes.c_int, [p, p, i64, i64, p, p, sz, p]),
         "eacb_scan_excl_i64": (ctypes.c_int, [p, p, i64, i64, p, p, sz, p]),
+        "eacb_tune_set": (ctypes.c_int, [ctypes.c_int, i64, i64, i64, i64, i64]),
+        "eacb_tune_clear": (None, []),
+        "eacb_tune_get": (i64, [ctypes.c_int, i64, i64, i64]),
         "eacb_debug_set_round_cap": (None, [ctypes.c_int]),
         "eacb_debug_set_round_team": (None, [ctypes.c_int]),
         "eacb_boruvka_workspace_size": (sz, [i32, i64]),
@@ -101,7 +104,53 @@ def load():
         f.restype = res
         f.argtypes = args
     _lib = L
+    if os.environ.get("EACB_TUNING", "1") != "0":
+        apply_tuning()
     return L
+
+
+# ---------------------------------------------------------------- tuning ---
+TUNING_PATH = os.path.join(_HERE, "tuning.json")
+TUNE_KNOBS = {"tc_ctas_per_sm": 0, "tc_buffers": 1, "co_count_ctas": 2, "co_fill_ctas": 3,
+              "mst_phase1_permille": 4, "round_team": 5}
+_tuning = {"python": {}, "applied": False}
+
+
+def apply_tuning(path=None):
+    """Loads the autotuner's table (masters_final_b200/tuning.json by
+    default) into the library's launch-shape table; entries the library
+    does not know are refused.  Returns the number of entries loaded."""
+    import json
+    L = load()
+    L.eacb_tune_clear()
+    _tuning["python"] = {}
+    _tuning["applied"] = False
+    path = path or TUNING_PATH
+    if not os.path.exists(path):
+        return 0
+    with open(path) as f:
+        table = json.load(f)
+    n = 0
+    for e in table.get("entries", []):
+        knob = TUNE_KNOBS[e["knob"]]
+        check(L.eacb_tune_set(knob, int(e["a"][0]), int(e["a"][1]), int(e["b"][0]),
+                              int(e["b"][1]), int(e["value"])), "tuning table")
+        n += 1
+    _tuning["python"] = dict(table.get("python", {}))
+    _tuning["applied"] = True
+    return n
+
+
+def clear_tuning():
+    """Back to the built-in launch shapes (the untuned configuration)."""
+    load().eacb_tune_clear()
+    _tuning["python"] = {}
+    _tuning["applied"] = False
+
+
+def tuned(name, default):
+    """A host-side tuned setting (e.g. the batched worker count)."""
+    return _tuning["python"].get(name, default)
 
 
 class Instance(ctypes.Structure):
@@ -198,14 +247,18 @@ def workspace(nbytes):
 
 def to_device(a, dtype=None):
     """numpy array or torch tensor -> contiguous CUDA tensor (no copy if
-    already there with the right dtype)."""
+    already there with the right dtype).  A pinned host tensor is copied
+    asynchronously on the current stream, which the library's calls use."""
     t = torch()
     if isinstance(a, t.Tensor):
         x = a
-        if dtype is not None:
+        if dtype is not None and x.dtype != dtype and x.is_cuda:
             x = x.to(dtype)
         if not x.is_cuda:
-            x = x.to(device())
+            pinned = x.is_pinned()
+            x = x.to(device(), non_blocking=pinned)
+            if dtype is not None and x.dtype != dtype:
+                x = x.to(dtype)
         return x.contiguous()
     arr = np.ascontiguousarray(a)
     x = t.from_numpy(arr)

@@ -274,6 +274,9 @@ extern "C" int eacb_batched_eac(eacb_instance *inst, int32_t n_inst,
         if (cudaSetDevice(dev) != cudaSuccess) return;
         cudaStream_t st = nullptr;
         if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return;
+        // instances run side by side: each one's Boruvka rounds take one
+        // block (a plain launch) instead of a cooperative grid over the GPU
+        if (nw > 1) eacb::set_thread_round_team(1);
         char *sl = base + (size_t)w * slice;
         for (;;) {
             const int32_t q = next.fetch_add(1);
@@ -288,6 +291,7 @@ extern "C" int eacb_batched_eac(eacb_instance *inst, int32_t n_inst,
             if (I.status == EACB_ERR_CUDA) I.cuda_error = eacb_last_cuda_error(nullptr, &I.cuda_line);
             if (I.status) cudaStreamSynchronize(st);   // nothing of it left in flight
         }
+        eacb::set_thread_round_team(0);
         cudaStreamDestroy(st);
     };
     std::vector<std::thread> pool;

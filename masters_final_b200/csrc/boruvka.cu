@@ -932,16 +932,17 @@ __host__ __device__ static int phase_ranges(const unsigned long long *hist, cons
 }
 
 // The weight phases of an MST on the device (no host read): ranges (lo, hi]
-// at cumulative fractions 1/8, 1/2, 1 of the histogram, one slot each in
-// lohi (an unused slot holds the empty range (255, 255]).
+// at cumulative fractions p1 (per mille of the entries; a tuning-table
+// knob, default a quarter) and 1 of the histogram, one slot each in lohi
+// (an unused slot holds the empty range (255, 255]).
 constexpr int kPhaseSlots = 2;
-__global__ void k_phase_plan(const unsigned long long *hist, int *lohi)
+__global__ void k_phase_plan(const unsigned long long *hist, int *lohi, int p1_permille)
 {
     __shared__ unsigned long long h[256];
     for (int b = threadIdx.x; b < 256; b += blockDim.x) h[b] = hist[b];
     __syncthreads();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const double fracs[kPhaseSlots] = {0.25, 1.0};
+    const double fracs[kPhaseSlots] = {p1_permille / 1000.0, 1.0};
     int lo[8], hi[8];
     const int np = phase_ranges(h, fracs, kPhaseSlots, lo, hi);
     for (int q = 0; q < kPhaseSlots; ++q) {
@@ -1575,6 +1576,10 @@ __global__ void k_rank_roots(const int32_t *parent, const int32_t *pos, int64_t 
 // g_round_team forces the number of participants (1 = one block).
 static int g_round_cap = 0;
 static int g_round_team = 0;
+// A host thread may cap the participants of the round kernels it launches
+// (set_thread_round_team): the batched path runs many small instances side
+// by side, each best served by a single block instead of the whole GPU.
+static thread_local int t_round_team_cap = 0;
 
 template <int MODE>
 static int round_team_max(int *out)
@@ -1593,16 +1598,19 @@ static int round_team_max(int *out)
     return EACB_OK;
 }
 
-// Participants for a graph of V0 vertices and at most Emax edge words: one
-// per 4096 vertices or 16K edge words, up to the resident maximum.
+// Participants for a graph of V0 vertices and about E edge words: one per
+// 4096 vertices or 16K edge words, up to the resident maximum.
 template <int MODE>
-static int round_team(int64_t V0, int64_t Emax, int *team)
+static int round_team(int64_t V0, int64_t E, int kind, int *team)
 {
     int mx = 1;
     int s = round_team_max<MODE>(&mx);
     if (s) return s;
-    const int64_t work = std::max((V0 + 4095) / 4096, (Emax + 16383) / 16384);
+    const int64_t work = std::max((V0 + 4095) / 4096, (E + 16383) / 16384);
     int t = g_round_team > 0 ? g_round_team : (int)std::min<int64_t>(work, mx);
+    const int64_t cap = g_round_team > 0 ? 0 : tune_get(TUNE_ROUND_TEAM, kind, V0, 0);
+    if (cap > 0) t = (int)std::min<int64_t>(t, cap);
+    if (t_round_team_cap > 0) t = std::min(t, t_round_team_cap);
     *team = std::max(1, std::min(t, mx));
     return EACB_OK;
 }
@@ -1664,6 +1672,7 @@ struct Engine {
     ScanScratch scan;
     int32_t V0;
     int64_t Emax;
+    int kind = 0;             // 0 graph MST/CC, 1 EAC final clustering (tuning shape)
 
     static Engine carve(Carver &c, int32_t V0, int64_t Emax)
     {
@@ -1726,10 +1735,10 @@ struct Engine {
     // with profiling on it is timed, and its algorithmic bytes come from the
     // per-round sizes the kernel records.
     template <int MODE>
-    int rounds(Pack pk, cudaStream_t st)
+    int rounds(Pack pk, cudaStream_t st, int64_t e_hint)
     {
         int team = 1;
-        int s = round_team<MODE>(V0, Emax, &team);
+        int s = round_team<MODE>(V0, e_hint, kind, &team);
         if (s) return s;
         RoundArgs a;
         a.pk = pk;
@@ -1798,7 +1807,7 @@ struct Engine {
             if (s) return s;
             k_phase_begin<<<1, 32, 0, st>>>(cnt, V0, q == 0 ? 1 : 0);
             EACB_CHECK_LAUNCH();
-            if ((s = rounds<SEL_MST>(pk, st))) return s;
+            if ((s = rounds<SEL_MST>(pk, st, Emax))) return s;
         }
         int64_t h[C_COUNT];
         int s = read_counts(st, h);
@@ -1884,7 +1893,7 @@ struct Engine {
     {
         k_set_sizes<<<1, 32, 0, st>>>(cnt, V_start, E0);
         EACB_CHECK_LAUNCH();
-        int s = rounds<MODE>(pk, st);
+        int s = rounds<MODE>(pk, st, E0);
         if (s) return s;
         int64_t h[C_COUNT];
         if ((s = read_counts(st, h))) return s;
@@ -1911,6 +1920,7 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
     int64_t h[C_COUNT];
     int64_t n_mst = 0, n_comp = 0;
     const unsigned gr = grid_for((int64_t)V * 32, 256);
+    const unsigned gph = grid_for(V, kPhThreads, 148 * 4);   // phase builds: grid-stride rows
     if (mode == SEL_MST) {
         // weight phases over the bucket histogram of the entries
         EACB_CUDA(cudaMemsetAsync(g.hist, 0, 256 * sizeof(unsigned long long), st));
@@ -1925,7 +1935,9 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
         }
         // the phase plan stays on the device: the whole MST is queued without
         // a host read until its end
-        k_phase_plan<<<1, 256, 0, st>>>(g.hist, g.lohi);
+        const int p1 = (int)std::min<int64_t>(999, std::max<int64_t>(
+                           1, tune_get(TUNE_MST_PHASE1, 0, V, 250)));
+        k_phase_plan<<<1, 256, 0, st>>>(g.hist, g.lohi, p1);
         EACB_CHECK_LAUNCH();
         std::vector<Phase> plan;
         for (int q = 0; q < kPhaseSlots; ++q) plan.push_back(Phase{0, 0, 0, V, q});
@@ -1939,7 +1951,9 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
                 EACB_CHECK_LAUNCH();
             }
             ProfScope ps(PROF_PHASE, st);
-            k_phase_csr<WT><<<gr, kPhThreads, 0, st>>>(
+            // the first phase reads every row and needs many warps to keep
+            // its loads in flight; the skipping phase touches few rows
+            k_phase_csr<WT><<<ph.slot == 0 ? gr : gph, kPhThreads, 0, st>>>(
                 first, deg, dest, weight, V, E, wbits, 0, 0, g.lohi, ph.slot, ph.slot == 0 ? 1 : 0,
                 ph.slot > 0 ? g.giant : nullptr, g.label, pk, g.ea,
                 (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best,
@@ -2131,6 +2145,10 @@ using namespace eacb;
 // EACB_ERR_NOT_CONVERGED, like the built-in one) and its participants
 // (0 = automatic, 1 = one block, more = that many cooperative blocks, at
 // most the resident maximum).  Process-wide; set them only between calls.
+namespace eacb {
+void set_thread_round_team(int blocks) { t_round_team_cap = blocks > 0 ? blocks : 0; }
+}  // namespace eacb
+
 extern "C" void eacb_debug_set_round_cap(int rounds) { g_round_cap = rounds > 0 ? rounds : 0; }
 extern "C" void eacb_debug_set_round_team(int blocks) { g_round_team = blocks > 0 ? blocks : 0; }
 
@@ -2298,6 +2316,7 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
     int32_t *cmin;
     carve_final(c, n, nnz, &g, &hist, &plan, &cmin);
     if (c.overflow) return EACB_ERR_WORKSPACE;
+    g.kind = 1;
     if ((s = g.reset(st))) return s;
     // 1. minimum spanning forest of the dissimilarity graph, by weight phases
     EACB_CUDA(cudaMemsetAsync(g.hist, 0, 256 * sizeof(unsigned long long), st));

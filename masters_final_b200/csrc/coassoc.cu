@@ -513,6 +513,7 @@ static int read_err(int *err, cudaStream_t st)
 
 static int row_grid(int ctas_per_sm = 2)
 {
+    ctas_per_sm = ctas_per_sm < 1 ? 1 : (ctas_per_sm > 2 ? 2 : ctas_per_sm);
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -584,7 +585,8 @@ extern "C" int eacb_coassoc_count(const int32_t *labels, int32_t n, int32_t P, i
     TailCtx tc{labels, w.members, w.mypos, w.S, n, P, K, w.ntiles};
     EACB_CUDA(allow_max_dyn_smem(k_rows_count));
     ProfScope ps(PROF_COASSOC, st);
-    k_rows_count<<<row_grid(), kRowThreads, kBitmapBytes, st>>>(
+    k_rows_count<<<row_grid((int)tune_get(TUNE_CO_COUNT_CTAS, P, n, 2)), kRowThreads, kBitmapBytes,
+                   st>>>(
         tc, w.order, w.rowperm, cap_indptr, w.rowcnt, w.rowflag, &w.queue[0], w.err);
     EACB_CHECK_LAUNCH();
     ps.done(0.0);
@@ -683,7 +685,8 @@ extern "C" int eacb_coassoc_fill(const int32_t *labels, int32_t n, int32_t P, in
     EACB_CUDA(allow_max_dyn_smem(k_rows_fill));
     EACB_CUDA(allow_max_dyn_smem(k_rows_capped));
     ProfScope ps(PROF_COASSOC, st);
-    k_rows_fill<<<row_grid(2), kFillThreads, kFillSmem, st>>>(
+    k_rows_fill<<<row_grid((int)tune_get(TUNE_CO_FILL_CTAS, P, n, 2)), kFillThreads, kFillSmem,
+                  st>>>(
         tc, w.rowperm, w.rowflag, indptr, indices, data, &w.queue[1], w.maxcnt, w.err);
     EACB_CHECK_LAUNCH();
     ps.done(0.0);

@@ -19,6 +19,21 @@ namespace eacb {
 inline void count_launch(int n = 1);
 // the calling thread's last failed CUDA runtime call (eacb_last_cuda_error)
 void note_cuda_error(int code, const char *file, int line);
+// caps the participants of the Boruvka round kernels this host thread
+// launches (0 = no cap)
+void set_thread_round_team(int blocks);
+// Launch-shape knobs of the tuning table (csrc/tune.cu); (a, b) is the
+// shape each user states.
+enum TuneKnob : int {
+    TUNE_TC_CTAS_PER_SM = 0,   // tensor-core labeler CTAs per SM (1, 2); a = d, b = n
+    TUNE_TC_BUFFERS = 1,       // its centroid tile buffers (1, 2); a = d, b = n
+    TUNE_CO_COUNT_CTAS = 2,    // co-association count pass CTAs per SM; a = P, b = n
+    TUNE_CO_FILL_CTAS = 3,     // co-association fill pass CTAs per SM; a = P, b = n
+    TUNE_MST_PHASE1 = 4,       // graph MST: first phase's share of the entries, per mille; a = 0, b = V
+    TUNE_ROUND_TEAM = 5,       // Boruvka round kernel participants at most; a = 0 graph, 1 EAC; b = V
+    TUNE_NKNOBS = 6
+};
+int64_t tune_get(int knob, int64_t a, int64_t b, int64_t dflt);
 }
 #define EACB_CUDA(call)                                           \
     do {                                                          \

@@ -25,6 +25,8 @@
 #include "kmeans_common.cuh"
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 namespace eacb {
 
 constexpr int kTM = 128;           // points per CTA tile
@@ -550,12 +552,17 @@ int label_pass_tc(const float *X, int32_t n, int32_t D, int32_t P, const float *
                            (16.0 * ((D + 15) / 16) + 4.0) * ldexp(1.0, -23);
     const float E = 2.f * (float)(dot_err + (D + 6) * ldexp(1.0, -24));
     const size_t a_bytes = (size_t)kTM * s.Kp * 2, b_bytes = (size_t)kTN * s.Kp * 2;
-    // double-buffer the centroid tiles only while two CTAs still fit per SM
-    const int nbuf = (a_bytes + 2 * b_bytes <= 110 * 1024) ? 2 : 1;
+    // CTAs per SM (two share the SM's 512 TMEM columns) and centroid tile
+    // buffers: tuning-table knobs; by default two CTAs, double-buffered while
+    // both still fit
+    const int ctas = tune_get(TUNE_TC_CTAS_PER_SM, D, n, 2) == 1 ? 1 : 2;
+    const size_t cap_bytes = ctas == 2 ? 110 * 1024 : 220 * 1024;
+    int nbuf = (a_bytes + 2 * b_bytes <= cap_bytes) ? 2 : 1;
+    nbuf = (int)std::min<int64_t>(nbuf, std::max<int64_t>(1, tune_get(TUNE_TC_BUFFERS, D, n, nbuf)));
     const size_t smem = a_bytes + nbuf * b_bytes;
-    // at least 100 KB so that no more than two CTAs (2 x 256 TMEM columns)
-    // share an SM
-    const size_t smem_req = smem < 100 * 1024 ? 100 * 1024 : smem;
+    // a floor on the request so that no more CTAs than asked share an SM
+    const size_t floor_bytes = ctas == 2 ? 100 * 1024 : 120 * 1024;
+    const size_t smem_req = smem < floor_bytes ? floor_bytes : smem;
     EACB_CUDA(allow_max_dyn_smem(k_label_tc));
     dim3 grid((unsigned)(s.n_pad / kTM), (unsigned)P);
     ProfScope ps(PROF_KMEANS, st);

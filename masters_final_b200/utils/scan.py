@@ -60,11 +60,21 @@ def exprefixsumNumba(in_ary, out_ary, init=0):
         _lib.check(_lib.load().eacb_workspace_status(_lib.ptr(ws), _lib.stream_handle()), "scan")
         return int(total.item())
     x = _lib.to_device(in_ary)
-    o = t.empty(x.numel(), dtype=getattr(t, np.dtype(out_ary.dtype).name), device=x.device)
+    o = t.empty(x.numel(), dtype=getattr(t, _lib.np_dtype_of(out_ary).name), device=x.device)
     total, ws = _scan(x, o, init)
-    out_ary[...] = o.cpu().numpy()
+    _to_host(o, out_ary)
     _lib.check(_lib.load().eacb_workspace_status(_lib.ptr(ws), _lib.stream_handle()), "scan")
     return int(total.item())
+
+
+def _to_host(dev, out):
+    """Copies a device result into the caller's host array (numpy, or a torch
+    CPU tensor -- pinned ones are written directly by the copy engine)."""
+    t = _lib.torch()
+    if isinstance(out, t.Tensor):
+        out.copy_(dev.view(out.shape))
+    else:
+        out[...] = dev.cpu().numpy().reshape(out.shape)
 
 
 def exprefixsumNumbaSingle(in_ary, init=0):
@@ -76,6 +86,6 @@ def exprefixsumNumbaSingle(in_ary, init=0):
         return int(total.item())
     x = _lib.to_device(in_ary)
     total, ws = _scan(x, x, init)
-    in_ary[...] = x.cpu().numpy()
+    _to_host(x, in_ary)
     _lib.check(_lib.load().eacb_workspace_status(_lib.ptr(ws), _lib.stream_handle()), "scan")
     return int(total.item())

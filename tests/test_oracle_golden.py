@@ -119,3 +119,50 @@ def test_eac_pipeline(name):
     nc, lab = oracle.sp_sl_lifetime(n, rows, ind.astype(np.int64), dia, int(g["P"]))
     assert nc == g["n_fclusts"]
     assert np.array_equal(lab, g["final_labels"])
+
+
+@pytest.mark.parametrize("name", ["eac_small", "eac_discard", "eac_10k"])
+def test_coassoc_rows_match_reference(name):
+    """The row-by-row restatement of the co-association build (used to check
+    sampled rows of matrices too large for the full restatement) gives the
+    reference's own rows, including rows that hit their capacity."""
+    g = golden(name)
+    L = g["labels_matrix"]
+    n = L.shape[1]
+    cap = oracle.indptr_linear(n, int(g["max_assocs"]))
+    if "indptr" in g:
+        ip, ind, dia = g["indptr"], g["indices"], g["diassoc"]
+    else:
+        # the 10k fixture keeps a digest of its matrix, which
+        # test_coassoc_10k_digest pins the full restatement to
+        ip, ind, cnt, _, _, _ = oracle.coassoc_build(L, cap)
+        dia = (cnt.max() + 1 - cnt).astype(np.uint8)
+    full = np.flatnonzero(np.diff(ip) == np.diff(cap))          # rows at capacity
+    rng = np.random.default_rng(5)
+    rows = np.unique(np.concatenate([rng.choice(n, min(n, 300), replace=False), full[:300]]))
+    const = None
+    for i, (cols, cnt) in zip(rows, oracle.coassoc_rows(L, cap, rows)):
+        s, e = ip[i], ip[i + 1]
+        assert np.array_equal(cols, ind[s:e])
+        tot = cnt.astype(np.int64) + dia[s:e].astype(np.int64)    # diassoc = max + 1 - count
+        if tot.size:
+            const = tot[0] if const is None else const
+            assert np.all(tot == const)
+    if name == "eac_discard":
+        assert full.size > 0
+
+
+def test_coassoc_10k_digest():
+    """The full restatement reproduces the reference's 10k-point matrix
+    (indptr, indices and dissimilarities, by digest) and counts."""
+    import hashlib
+    g = golden("eac_10k")
+    L = g["labels_matrix"]
+    n = L.shape[1]
+    ip, ind, cnt, nnz, disc, st = oracle.coassoc_build(L, oracle.indptr_linear(n, int(g["max_assocs"])))
+    assert st == 0 and nnz == g["nnz"] and disc == g["nnz_discarded"]
+    dia = (cnt.max() + 1 - cnt).astype(np.uint8)
+    h = hashlib.sha256()
+    for a in (ip, ind, dia):
+        h.update(np.ascontiguousarray(a).tobytes())
+    assert h.hexdigest() == str(g["coassoc_sha"])
