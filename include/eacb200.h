@@ -148,7 +148,9 @@ int eacb_scan_excl_i32_noalloc(const int32_t *in, int32_t *out, int64_t n, int64
  * Replaces MyML/MyML/graph/mst.py:417-564 (boruvka_minho_gpu) and its
  * kernels :574-809.  Graph: row r has the entries [first_edge[r],
  * first_edge[r] + out_degree[r]) of dest/weight; every undirected edge is
- * stored in both directions; self loops are ignored.
+ * stored in both directions (a graph with unequal numbers of entries u -> v
+ * with u < v and with u > v returns EACB_ERR_BAD_INPUT); self loops are
+ * ignored.
  * Ties are broken by the strict order (weight, min(u,v), max(u,v)), so the
  * forest is unique.  mst_out (capacity n_vertices - 1) receives, per chosen
  * edge, the index of its entry in row min(u,v) (the smallest such index with

@@ -5,14 +5,14 @@
 // MyML/MyML/graph/connected_components.py:176-345, MyML/MyML/EAC/eac.py:199-391.
 //
 // Design (not the reference's):
-//  * Every directed edge is ONE 64-bit word: weight-order bits | min(u,v) |
-//    max(u,v) | direction bit, with u, v the ORIGINAL endpoints.  A round
-//    never rewrites edges; it only drops the ones that became internal.  The
-//    current endpoints are label[u], label[v] (label = original vertex ->
-//    current supervertex, kept for all original vertices, L2 resident).
+//  * Every undirected edge is ONE 64-bit word: weight-order bits | min(u,v) |
+//    max(u,v) | 0, with u, v the ORIGINAL endpoints, offered to the selection
+//    slots of both its ends.  A round never rewrites edges; it only drops the
+//    ones that became internal.  The current endpoints are the roots of u
+//    and v in a union-find forest over the original vertices.
 //  * Min-edge selection is an atomicMin of a 64-bit selection key per
 //    supervertex: (weight, min, max) for the MST -- a strict total order, so
-//    the forest is unique -- or (weight, destination supervertex) for the
+//    the forest is unique -- or (weight, other end's supervertex) for the
 //    reference's connected-components numbering.  Lanes of a warp holding
 //    edges of the same supervertex are pre-reduced with a segmented shuffle
 //    scan, so one atomic is issued per run, not per edge.
@@ -130,7 +130,7 @@ constexpr int64_t kETile = (int64_t)kET * kEI;
 // Each source splits an edge into fetch() (independent global loads, issued
 // for all items of a thread before any is used) and resolve() (the dependent
 // work), so a thread keeps all its loads in flight at once.
-// Both directions of undirected keys (MST selection keys) below a weight cap
+// Undirected keys (MST selection keys) below a weight cap, one word each
 struct SrcForest {
     typedef uint64_t Raw;
     const uint64_t *keys;   // selection keys (w, a, b)
@@ -168,7 +168,7 @@ __device__ __forceinline__ bool resolve_item<SrcForest>(const SrcForest &src, co
                                                         int64_t i, uint64_t &k, int32_t &su,
                                                         int32_t &sv, uint32_t &w)
 {
-    return src.resolve_dir(r, i >= src.n_keys, k, su, sv, w);
+    return src.resolve_dir(r, false, k, su, sv, w);
 }
 
 // Tile kernel: keep-filter + order-preserving compaction + fused min-edge
@@ -223,6 +223,11 @@ k_edge_tile(Src src, int64_t n_in, uint64_t *eout, unsigned long long *best,
         const uint64_t sel =
             MODE == SEL_MST ? (k[it] >> 1) : (((uint64_t)w[it] << 32) | (uint32_t)sv[it]);
         seg_min_atomic(keep[it], su[it], sel, best);
+        // the word stands for both directions: the other end's offer
+        if (keep[it])
+            min_if_lower(&best[sv[it]],
+                         MODE == SEL_MST ? (k[it] >> 1)
+                                         : (((uint64_t)w[it] << 32) | (uint32_t)su[it]));
     }
     __syncthreads();
     if (warp == 0) {
@@ -269,46 +274,6 @@ k_edge_tile(Src src, int64_t n_in, uint64_t *eout, unsigned long long *best,
     }
     if (!d_n) return;            // one tile per block
     __syncthreads();             // shared state is reused by the next tile
-    }
-}
-
-// Round-0 edges straight from a symmetric CSR, one warp per row: entry e
-// becomes edge word e (a self loop or an entry outside every row stays a dead
-// word, dropped by the first contraction); the row's minimum selection key is
-// one atomicMin.
-template <int MODE, typename WT>
-__global__ void k_edges_csr(const int32_t *first, const int32_t *deg, const int32_t *dest,
-                            const WT *weight, int32_t V, int64_t E, Pack pk, uint64_t *eout,
-                            unsigned long long *best, int *err)
-{
-    const int lane = threadIdx.x & 31;
-    for (int64_t u = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < V;
-         u += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int64_t f = first[u], d = deg[u];
-        if (f < 0 || d < 0 || f + d > E) {
-            if (lane == 0) set_err(err, DEV_BAD_INPUT);
-            continue;
-        }
-        uint64_t m = kNone;
-        for (int64_t e = f + lane; e < f + d; e += 32) {
-            const int32_t v = dest[e];
-            if (v < 0 || v >= V) {
-                set_err(err, DEV_BAD_INPUT);
-                continue;
-            }
-            if (v == (int32_t)u) continue;          // self loop: stays dead
-            const uint32_t w = wword(weight[e]);
-            const uint64_t k = pk.make(w, (uint32_t)u, (uint32_t)v);
-            eout[e] = k;
-            const uint64_t sel = MODE == SEL_MST ? (k >> 1) : (((uint64_t)w << 32) | (uint32_t)v);
-            m = sel < m ? sel : m;
-        }
-#pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) {
-            const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
-            m = x < m ? x : m;
-        }
-        if (lane == 0 && m != kNone) atomicMin(&best[u], (unsigned long long)m);
     }
 }
 
@@ -515,20 +480,23 @@ __device__ __forceinline__ void phase_stage(bool keep, uint64_t k, uint64_t *sta
 }
 
 // identity: the first phase (every vertex its own root: no label is read,
-// and every entry is checked once for a destination out of range).
+// and every entry is checked once for a destination out of range, and
+// counted into sym[0] (u < v) or sym[1] (u > v): a symmetric graph has as
+// many of each).
 // skip_root (device int, or null; -1 = none): a later phase skips the rows of
 // that root -- the giant component the earlier phases built -- and emits
 // both directions of each kept entry whose other end lies in it, so the
 // giant still sees every edge it has to another component (each such edge is
 // found once, from the row outside the giant).
-template <typename WT>
+template <int MODE, typename WT>
 __global__ void __launch_bounds__(kPhThreads)
 k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const WT *weight,
             int32_t V, int64_t E, int wbits, int lo, int hi, const int *dev_lohi, int slot,
             int identity, const int32_t *skip_root, const int32_t *label, Pack pk,
             uint64_t *eout, unsigned long long *cursor, unsigned long long cap,
-            unsigned long long *best, int *err)
+            unsigned long long *best, unsigned long long *sym, int *err)
 {
+    unsigned long long n_lt = 0, n_gt = 0;   // this lane's entries by direction
     if (dev_lohi) {
         lo = dev_lohi[2 * slot];
         hi = dev_lohi[2 * slot + 1];
@@ -541,19 +509,20 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
     uint64_t *stage = stage_all[warp];
     const int64_t step = (int64_t)kPhWarps * 32;
     auto root_of = [&](int32_t v) -> int32_t { return identity ? v : label[v]; };
-    // emits the kept entry u -> v (roots lu != lv): its word, offered to lu,
-    // and when v's root is the skipped giant, the reverse word, offered to it
-    auto emit = [&](bool keep, uint32_t w, int32_t u, int32_t v, int32_t lu, int32_t lv,
+    // a kept entry u -> v (roots lu != lv) becomes one word for the
+    // undirected edge: written from the row of its smaller end, or from the
+    // only row read when v lies in the skipped giant; its key is offered to
+    // both ends (MST: (weight, min, max); CC: (weight, other end's root))
+    auto emit = [&](bool kept, uint32_t w, int32_t u, int32_t v, int32_t lu, int32_t lv,
                     int &cnt) {
+        const bool keep = kept && (u < v || lv == skip);
         const uint64_t k = keep ? pk.make(w, (uint32_t)u, (uint32_t)v) : 0ull;
         phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
-        if (keep) min_if_lower(&best[lu], k >> 1);
-        if (skip >= 0) {
-            const bool rev = keep && lv == skip;
-            if (__any_sync(0xffffffffu, rev)) {
-                phase_stage(rev, k ^ 1ull, stage, cnt, eout, cursor, cap, err);
-                if (rev) min_if_lower(&best[skip], k >> 1);
-            }
+        if (keep) {
+            min_if_lower(&best[lu],
+                         MODE == SEL_MST ? (k >> 1) : (((uint64_t)w << 32) | (uint32_t)lv));
+            min_if_lower(&best[lv],
+                         MODE == SEL_MST ? (k >> 1) : (((uint64_t)w << 32) | (uint32_t)lu));
         }
     };
     for (int64_t r0 = (int64_t)blockIdx.x * step; r0 < V; r0 += (int64_t)gridDim.x * step) {
@@ -626,6 +595,7 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
                             if (v[q] < 0 || v[q] >= V) {
                                 set_err(err, DEV_BAD_INPUT);
                             } else if (v[q] != (int32_t)(u0 + r[q])) {
+                                if (v[q] > (int32_t)(u0 + r[q])) ++n_lt; else ++n_gt;
                                 const int bk = (int)wbucket(w[q], wbits);
                                 cand[q] = bk > lo && bk <= hi;
                             }
@@ -654,6 +624,7 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
                             if (v < 0 || v >= V) {
                                 set_err(err, DEV_BAD_INPUT);
                             } else if (v != u) {
+                                if (v > u) ++n_lt; else ++n_gt;
                                 w = wword(weight[e]);
                                 const int bk = (int)wbucket(w, wbits);
                                 cand = bk > lo && bk <= hi;
@@ -672,6 +643,14 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
             for (int i = lane; i < cnt; i += 32) eout[at + i] = stage[i];
         }
         __syncthreads();          // staging and s_cnt are reused by the next step
+    }
+    if (sym) {
+        n_lt = __reduce_add_sync(0xffffffffu, (unsigned)n_lt);
+        n_gt = __reduce_add_sync(0xffffffffu, (unsigned)n_gt);
+        if ((threadIdx.x & 31) == 0 && (n_lt | n_gt)) {
+            atomicAdd(&sym[0], n_lt);
+            atomicAdd(&sym[1], n_gt);
+        }
     }
 }
 
@@ -719,18 +698,18 @@ k_pick_giant(const int32_t *label, int64_t V0, int32_t *out)
     }
 }
 
-// Same for an upper-triangle CSR with uint8 weights: both directions of each
-// kept entry.  Co-association rows are long (thousands of entries), so a
+// Same for an upper-triangle CSR with uint8 weights: one word per kept entry,
+// offered to both ends.  Co-association rows are long (thousands of entries), so a
 // warp takes one row and walks it in 128-entry groups, each lane taking four
 // consecutive entries: their four weights (one word) are read first, and the
 // four column indices (16 bytes) only when one of the weights falls in the
 // phase's range, so a phase over a narrow range reads little more than the
 // weight array; only those entries gather the other end's label.  A first
 // walk (four groups in flight) counts the kept entries, the warp reserves
-// 2 x that many words with one atomic, and a second walk over the (now
-// cached) row writes them: per group its i -> j words, then its j -> i words,
-// runs of equal source for the min-edge selection of later rounds.  Each
-// entry is checked (j > i, j < n) in the phase whose range holds its weight.
+// that many words with one atomic, and a second walk over the (now cached)
+// row writes them, runs of equal first end for the min-edge selection of
+// later rounds.  Each entry is checked (j > i, j < n) in the phase whose
+// range holds its weight.
 __global__ void __launch_bounds__(kPhThreads, 4)
 k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, int32_t n,
               int64_t nnz, int lo, int hi, int dense, int64_t row0, int64_t row1,
@@ -842,9 +821,9 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
         cnt = __reduce_add_sync(0xffffffffu, cnt);
         if (cnt == 0) continue;
         unsigned long long at = 0;
-        if (lane == 0) at = atomicAdd(cursor, 2ull * (unsigned long long)cnt);
+        if (lane == 0) at = atomicAdd(cursor, (unsigned long long)cnt);
         at = __shfl_sync(0xffffffffu, at, 0);
-        if (at + 2ull * (unsigned long long)cnt > cap) {
+        if (at + (unsigned long long)cnt > cap) {
             if (lane == 0) set_err(err, DEV_CAPACITY);
             continue;
         }
@@ -872,12 +851,11 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
                 if (!((km >> q) & 1u)) continue;
                 const uint64_t k = pk.make((wv >> (8 * q)) & 255u, (uint32_t)i, (uint32_t)jj[q]);
                 eout[p] = k;
-                eout[p + tot] = k | 1ull;
                 m = (k >> 1) < m ? (k >> 1) : m;
                 min_if_lower(&best[lj[q]], k >> 1);
                 ++p;
             }
-            at += 2ull * (unsigned long long)tot;
+            at += (unsigned long long)tot;
         }
 #pragma unroll
         for (int o = 16; o >= 1; o >>= 1) {
@@ -984,6 +962,8 @@ enum : int {
     C_EBUF = 7,       // edge buffer holding the last round's survivors (0 or 1)
     C_AUX0 = 8,       // scratch totals of single-pass kernels
     C_AUX1 = 9,
+    C_SYM_LT = 10,    // CSR entries u -> v with u < v (symmetry check)
+    C_SYM_GT = 11,    // ... with u > v
     C_COUNT = 16
 };
 
@@ -1040,8 +1020,8 @@ __global__ void k_set_sizes(int64_t *cnt, int64_t V, int64_t E)
 //      edge word whose endpoints now have different roots stays in its
 //      segment (compacted in place: a tile's words are in registers before
 //      any of the tile's survivors is written, and survivors never move past
-//      their tile) and is offered to its source root's slot (one atomicMin
-//      per run of equal source in a warp).  Edge order does not matter:
+//      their tile) and is offered to both its roots' slots (one atomicMin per
+//      run of equal first root in a warp, and one for the other root).  Edge order does not matter:
 //      selection uses total orders, so every result is independent of it.
 // Three barriers per round.  After the last one every participant reads the
 // same sizes and takes the same decision to stop:
@@ -1401,8 +1381,8 @@ k_rounds(RoundArgs a)
                 for (int it = 0; it < kRItems; ++it) {
                     ok[it] = k[it] != kNone && a.pk.a(k[it]) < (uint64_t)a.V0 &&
                              a.pk.b(k[it]) < (uint64_t)a.V0;
-                    ep[2 * it] = ok[it] ? (int32_t)a.pk.src(k[it]) : -1;
-                    ep[2 * it + 1] = ok[it] ? (int32_t)a.pk.dst(k[it]) : -2;
+                    ep[2 * it] = ok[it] ? (int32_t)a.pk.a(k[it]) : -1;
+                    ep[2 * it + 1] = ok[it] ? (int32_t)a.pk.b(k[it]) : -2;
                 }
                 find_batch<2 * kRItems>(a.parent, ep, a.err);
                 bool keep[kRItems];
@@ -1413,10 +1393,16 @@ k_rounds(RoundArgs a)
                     keep[it] = ok[it] && su != sv;
                     bal[it] = __ballot_sync(0xffffffffu, keep[it]);
                     if (lane == 0) s_off[it][warp] = __popc(bal[it]);
+                    // one word per undirected edge: offered to both ends
                     const uint64_t sel = MODE == SEL_MST
                                              ? (k[it] >> 1)
                                              : (((uint64_t)a.pk.w(k[it]) << 32) | (uint32_t)sv);
                     seg_min_atomic(keep[it], su, sel, a.best);
+                    if (keep[it])
+                        min_if_lower(&a.best[sv],
+                                     MODE == SEL_MST
+                                         ? (k[it] >> 1)
+                                         : (((uint64_t)a.pk.w(k[it]) << 32) | (uint32_t)su));
                 }
                 __syncthreads();                // the tile's words are all read
                 if (warp == 0) {
@@ -1953,11 +1939,11 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
             ProfScope ps(PROF_PHASE, st);
             // the first phase reads every row and needs many warps to keep
             // its loads in flight; the skipping phase touches few rows
-            k_phase_csr<WT><<<ph.slot == 0 ? gr : gph, kPhThreads, 0, st>>>(
+            k_phase_csr<SEL_MST, WT><<<ph.slot == 0 ? gr : gph, kPhThreads, 0, st>>>(
                 first, deg, dest, weight, V, E, wbits, 0, 0, g.lohi, ph.slot, ph.slot == 0 ? 1 : 0,
                 ph.slot > 0 ? g.giant : nullptr, g.label, pk, g.ea,
                 (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best,
-                g.err);
+                ph.slot == 0 ? (unsigned long long *)&g.cnt[C_SYM_LT] : nullptr, g.err);
             EACB_CHECK_LAUNCH();
             // compulsory reads: row extents and labels (12 B per row), dest and
             // weight (4 + sizeof(WT) B per entry); the written words follow
@@ -1966,14 +1952,18 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
         };
         if ((s = g.run_phased(pk, plan, build, st, &n_mst, &n_comp))) return s;
     } else {
+        // every entry with identity labels: one word per undirected edge and
+        // each vertex's first selection (the reference's round one)
         if (E > 0) {
-            // dead words everywhere first: entries outside every row, self loops
-            EACB_CUDA(cudaMemsetAsync(g.ea, 0xff, sizeof(uint64_t) * E, st));
-            k_edges_csr<SEL_CC, WT><<<gr, 256, 0, st>>>(first, deg, dest, weight, V, E, pk, g.ea,
-                                                        g.best, g.err);
+            k_phase_csr<SEL_CC, WT><<<gr, kPhThreads, 0, st>>>(
+                first, deg, dest, weight, V, E, wbits, -1, 255, nullptr, 0, 1, nullptr, g.label, pk,
+                g.ea, (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best,
+                (unsigned long long *)&g.cnt[C_SYM_LT], g.err);
             EACB_CHECK_LAUNCH();
         }
-        if ((s = g.run<SEL_CC>(pk, E, V, st, &n_mst, &n_comp))) return s;
+        if ((s = g.read_counts(st, h))) return s;
+        if (h[C_SYM_LT] != h[C_SYM_GT]) return EACB_ERR_BAD_INPUT;   // not symmetric
+        if ((s = g.run<SEL_CC>(pk, h[C_CURSOR], V, st, &n_mst, &n_comp))) return s;
     }
     if (mode == SEL_MST) {
         if (n_mst > 0) {
@@ -1982,6 +1972,7 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
             EACB_CHECK_LAUNCH();
         }
         if ((s = g.read_counts(st, h))) return s;
+        if (h[C_SYM_LT] != h[C_SYM_GT]) return EACB_ERR_BAD_INPUT;   // not symmetric
         *host_n_mst = n_mst;
     } else {
         // the reference's component numbers: ranks of the root ids
@@ -2182,14 +2173,21 @@ extern "C" int eacb_connected_components(const int32_t *dest, const void *weight
                         n_edges, nullptr, &dummy, labels, host_n_comps, ws, ws_bytes, stream);
 }
 
-// Edge words of the final clustering: every entry's two directions when the
-// matrix is small, else 256 words per point (at least 2^20): room for the
-// usual output of a phase, not its worst case (a phase that overflows is
+// Matrices of up to this many entries get an edge word for every entry, so
+// no phase can overflow and all phases are queued with no host read between
+// them (the many small matrices of batched EAC); larger ones keep the
+// bounded edge array below and may redo an overflowing phase in pieces.
+constexpr int64_t kFinalQueuedEntries = (int64_t)1 << 26;
+
+// Edge words of the final clustering (one per kept entry): every entry when
+// the matrix is small, else 256 words per point (at least 2^20): room for
+// the usual output of a phase, not its worst case (a phase that overflows is
 // redone in pieces), so a matrix of thousands of entries per row does not
 // need an edge array of its own size.
 static int64_t final_edge_cap(int32_t n, int64_t nnz)
 {
-    const int64_t all = 2 * (nnz > (int64_t)n ? nnz : (int64_t)n);
+    const int64_t all = nnz > (int64_t)n ? nnz : (int64_t)n;
+    if (all <= kFinalQueuedEntries) return all;       // nothing can overflow
     const int64_t usual = 256 * (int64_t)n > ((int64_t)1 << 20) ? 256 * (int64_t)n : ((int64_t)1 << 20);
     return all < usual ? all : usual;
 }
@@ -2354,9 +2352,13 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
     };
     std::vector<int64_t> hip;
     auto split = [&](const Phase &ph, const unsigned long long kh[256], std::vector<Phase> &out) {
-        return split_final_phase(ph, kh, g.Emax / 2, indptr, n, hip, st, out);
+        return split_final_phase(ph, kh, g.Emax, indptr, n, hip, st, out);
     };
-    if ((s = g.run_phased_retry(pk, phases, build, split, st, &n_mst, &n_comp))) return s;
+    if (g.Emax >= nnz) {
+        if ((s = g.run_phased(pk, phases, build, st, &n_mst, &n_comp))) return s;
+    } else {
+        if ((s = g.run_phased_retry(pk, phases, build, split, st, &n_mst, &n_comp))) return s;
+    }
     // 2. lifetime rule on the weight histogram
     EACB_CUDA(cudaMemsetAsync(hist, 0, 256 * sizeof(int64_t), st));
     if (n_mst > 0) {
@@ -2375,11 +2377,11 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
         *host_n_fclusts = 1;
         return EACB_OK;
     }
-    // 3. components of the forest without the cut edges: both directions of
-    //    the kept forest keys go from mst into ea, then the rounds
+    // 3. components of the forest without the cut edges: the kept forest
+    //    keys go from mst into ea, then the rounds
     if ((s = g.reset(st))) return s;
     SrcForest sf{g.mst, n_mst, hp.wmax, pk};
-    if ((s = g.filter<SEL_CC>(sf, 2 * n_mst, g.ea, st))) return s;
+    if ((s = g.filter<SEL_CC>(sf, n_mst, g.ea, st))) return s;
     int64_t h[C_COUNT];
     if ((s = g.read_counts(st, h))) return s;
     int64_t nm2 = 0, nc2 = 0;

@@ -212,7 +212,7 @@ def test_final_clustering_capacity_split_phases(T):
     from masters_final_b200.EAC.eac import sp_sl_lifetime_csr
     rng = np.random.default_rng(8)
     n = 12_000
-    m = 2_600_000                                   # 2 m words > the edge array (256 n)
+    m = 4_000_000                                   # ~3.7M entries > the edge array (256 n words)
     a = rng.integers(0, n - 1, m)
     b = a + 1 + (rng.random(m) * (n - 1 - a)).astype(np.int64)
     key = np.unique(a * n + b)
@@ -239,15 +239,15 @@ def test_final_clustering_overflow_retry(T):
     from masters_final_b200 import _lib
     from masters_final_b200.EAC.eac import sp_sl_lifetime_csr
     rng = np.random.default_rng(12)
-    n = 2000
+    n = 2400
     a, b = np.triu_indices(n, 1)
-    m = a.size                                      # 1,999,000 entries
-    group = rng.integers(0, 3, n)                   # three groups joined by heavy entries
+    m = a.size                                      # 2,878,800 entries
+    group = rng.integers(0, 2, n)                   # two groups joined by heavy entries
     inside = group[a] == group[b]
     w = np.where(inside, rng.integers(3, 60, m), rng.integers(150, 200, m)).astype(np.uint8)
     pick = rng.permutation(np.nonzero(inside)[0])
     w[pick[:10_000]] = 1
-    w[pick[10_000:610_000]] = 2                     # 600k entries: 1.2M words > 2^20
+    w[pick[10_000:1_210_000]] = 2                   # 1.2M entries (words) > 2^20
     L = _lib.load()
     assert L.eacb_final_clustering_workspace_size(n, m) < 8 * 2 * m
     indptr = np.zeros(n + 1, dtype=np.int64)
