@@ -153,9 +153,9 @@ def measured_peak():
 # algorithmic bytes per launch)
 ROOF_KERNELS = [
     (0, "k_rounds (every Boruvka round of a weight phase in one persistent kernel)",
-     "per round: 8 B per edge word read + 8 B per surviving word written + 8 B per original "
-     "vertex (label read and written) + 24 B per supervertex (selection slot, successor, "
-     "new id)"),
+     "per round: 16 B per edge word (the word and its two endpoints' parents) + 8 B per "
+     "surviving word written back + 20 B per active root (list entry, selection slot, "
+     "successor, parent)"),
     (4, "k_phase_csr (weight-phase edge build + first min-edge selection)",
      "12 B per vertex (row extent, label) + 5 B per CSR entry (dest, uint8 weight) "
      "+ 8 B per edge word written"),
