@@ -3,6 +3,7 @@
 PyTorch is used only for device buffers and streams.  There is no fallback:
 if the library or a CUDA device is missing, every entry point raises.
 """
+import contextlib
 import ctypes
 import os
 
@@ -112,7 +113,7 @@ def load():
 # ---------------------------------------------------------------- tuning ---
 TUNING_PATH = os.path.join(_HERE, "tuning.json")
 TUNE_KNOBS = {"tc_ctas_per_sm": 0, "tc_buffers": 1, "co_count_ctas": 2, "co_fill_ctas": 3,
-              "mst_phase1_permille": 4, "round_team": 5}
+              "mst_phase1_permille": 4, "round_team": 5, "co_dense_ratio": 6}
 _tuning = {"python": {}, "applied": False}
 
 
@@ -120,12 +121,15 @@ def apply_tuning(path=None):
     """Loads the autotuner's table (masters_final_b200/tuning.json by
     default) into the library's launch-shape table; entries the library
     does not know are refused.  Returns the number of entries loaded."""
-    import json
     L = load()
     L.eacb_tune_clear()
     _tuning["python"] = {}
     _tuning["applied"] = False
-    path = path or TUNING_PATH
+    return _add_table(L, path or TUNING_PATH)
+
+
+def _add_table(L, path):
+    import json
     if not os.path.exists(path):
         return 0
     with open(path) as f:
@@ -139,6 +143,25 @@ def apply_tuning(path=None):
     _tuning["python"] = dict(table.get("python", {}))
     _tuning["applied"] = True
     return n
+
+
+@contextlib.contextmanager
+def forced(name, value):
+    """Within the block the knob `name` takes `value` for every shape (an
+    entry ahead of the loaded table); the table is reloaded afterwards."""
+    L = load()
+    was = _tuning["applied"]
+    L.eacb_tune_clear()
+    check(L.eacb_tune_set(TUNE_KNOBS[name], 0, 1 << 62, 0, 1 << 62, int(value)), "tuning table")
+    if was:
+        _add_table(L, TUNING_PATH)
+    try:
+        yield
+    finally:
+        if was:
+            apply_tuning()
+        else:
+            clear_tuning()
 
 
 def clear_tuning():

@@ -35,6 +35,8 @@
 #include "scan_impl.cuh"
 #include "members.cuh"
 
+#include <cuda_fp16.h>
+
 namespace eacb {
 
 constexpr int kMaxK = 8192;            // largest cluster id + 1 supported
@@ -52,6 +54,22 @@ constexpr int kFillSmem = kCountBytes + kCountBytes / 16;
 constexpr int kCapCols = 16 * 1024;            // capped rows: columns per chunk
 constexpr int kCapSmem = kCapCols * 5;         // byte counters + 32-bit ranks
 constexpr int kMaxP = 255;
+// work queues: 0 count rows, 1 fill rows, 2 capped rows, 3 row order,
+// 4 neighbourhoods, 5 pair tiles (count), 6 pair tiles (fill)
+constexpr int kQueues = 8;
+
+// pair tiles: 128 rows x 128 columns, labels as FP16 pairs (exact below 2048)
+constexpr int kPT = 128;
+constexpr int kPairThreads = 256;
+constexpr int kDenseMaxK = 2048;
+constexpr int kNbrThreads = 512;
+constexpr int kNbrBytes = 64 * 1024;           // neighbourhood chunk: 524,288 columns
+constexpr int kMaxGroupLists = 4096;           // (partition, cluster) lists per group
+constexpr int kNbrSmem = kNbrBytes + kMaxGroupLists * (8 + 8 + 4);
+constexpr int64_t kDenseRatioDefault = 16;
+
+// half2 words per point in the FP16 label copy: P rounded up to 8 partitions
+__host__ __device__ constexpr int32_t pair_words(int32_t P) { return ((P + 7) / 8) * 4; }
 
 struct CoWS {
     int *err;
@@ -62,18 +80,32 @@ struct CoWS {
     int32_t *ncl;         // P non-empty clusters
     int32_t *order;       // P processing order
     int32_t *rowcnt;      // n kept columns per row
-    int32_t *rowflag;     // n: 1 = distinct columns exceed the capacity
+    int32_t *rowflag;     // n: bit 0 = distinct columns exceed the capacity,
+                          //    bit 1 = the row's group takes the pair tiles
     int32_t *rowperm;     // n: the order the row kernels take rows in
-    int *queue;           // 4 row-queue counters
+    int *queue;           // work-queue counters
     unsigned long long *disc;   // discarded counts
     int *maxcnt;          // largest kept count
+    int *prow;            // the partition whose clusters order the rows
+    uint32_t *lt;         // n x Q: FP16 label pairs, point-major (pair tiles)
+    int64_t *grp_off;     // K: a group's neighbourhood in nbr
+    int32_t *grp_len;     // K: its length
+    int32_t *grp_tiles;   // K (+1): pair-tile row blocks of a group (0: streamed)
+    int64_t *grp_item0;   // K + 1: exclusive scan of grp_tiles
+    int32_t *nbr;         // neighbourhoods, back to back
+    unsigned long long *nbr_used;
+    int32_t *rowlist;     // n: rows a streaming kernel takes
+    int *rowlist_n;
     ScanScratch scan;
-    int64_t ntiles;
+    int64_t ntiles, nbr_cap;
+    int32_t Q;            // half2 words per point in lt
     static CoWS carve(Carver &c, int32_t n, int32_t P, int32_t K)
     {
         CoWS w;
         w.err = c.take<int>(1);
         w.ntiles = ((int64_t)n + kMLTile - 1) / kMLTile;
+        w.Q = pair_words(P);
+        w.nbr_cap = 16 * (int64_t)n + 65536;
         const int64_t pn = (int64_t)P * n;
         const int64_t m = (int64_t)P * K * w.ntiles;
         w.members = c.take<int32_t>(pn > 0 ? pn : 1);
@@ -85,9 +117,19 @@ struct CoWS {
         w.rowcnt = c.take<int32_t>(n);
         w.rowflag = c.take<int32_t>(n);
         w.rowperm = c.take<int32_t>(n);
-        w.queue = c.take<int>(4);
+        w.queue = c.take<int>(kQueues);
         w.disc = c.take<unsigned long long>(1);
         w.maxcnt = c.take<int>(1);
+        w.prow = c.take<int>(1);
+        w.lt = c.take<uint32_t>((size_t)n * w.Q);
+        w.grp_off = c.take<int64_t>(K);
+        w.grp_len = c.take<int32_t>(K);
+        w.grp_tiles = c.take<int32_t>((size_t)K + 1);
+        w.grp_item0 = c.take<int64_t>((size_t)K + 1);
+        w.nbr = c.take<int32_t>(w.nbr_cap);
+        w.nbr_used = c.take<unsigned long long>(1);
+        w.rowlist = c.take<int32_t>(n);
+        w.rowlist_n = c.take<int>(1);
         w.scan = ScanScratch::carve(c, m + 1 > n ? m + 1 : n, w.err);
         return w;
     }
@@ -177,18 +219,19 @@ __device__ __forceinline__ void stream_chunk(const int32_t *members, int64_t *ts
 
 // ---------------------------------------------------------------- pass 1 --
 __global__ void __launch_bounds__(kRowThreads)
-k_rows_count(TailCtx tc, const int32_t *order, const int32_t *rowperm, const int64_t *cap_indptr,
-             int32_t *rowcnt, int32_t *rowflag, int *queue, int *err)
+k_rows_count(TailCtx tc, const int32_t *order, const int32_t *rows, const int *nrows,
+             const int64_t *cap_indptr, int32_t *rowcnt, int32_t *rowflag, int *queue, int *err)
 {
     extern __shared__ uint32_t bm[];
     __shared__ int64_t ts[kMaxP], te[kMaxP];
     __shared__ int s_row, s_next;
     const int32_t n = tc.n, P = tc.P;
+    const int nr = *nrows;
     constexpr int32_t kCols = kBitmapBytes * 8;
     while (true) {
         const int qi = next_row(queue, &s_row);
-        if (qi >= n) break;
-        const int i = rowperm[qi];
+        if (qi >= nr) break;
+        const int i = rows[qi];
         const int64_t cap = cap_indptr[i + 1] - cap_indptr[i];
         for (int p = threadIdx.x; p < P; p += blockDim.x) {
             int64_t s, e;
@@ -282,8 +325,8 @@ __device__ __forceinline__ int64_t emit_flagged(uint32_t *ctr32, uint32_t *flag3
 }
 
 __global__ void __launch_bounds__(kFillThreads, 2)
-k_rows_fill(TailCtx tc, const int32_t *rowperm, const int32_t *rowflag, const int64_t *indptr,
-            int32_t *indices, uint8_t *data, int *queue, int *gmax, int *err)
+k_rows_fill(TailCtx tc, const int32_t *rows, const int *nrows, const int32_t *rowflag,
+            const int64_t *indptr, int32_t *indices, uint8_t *data, int *queue, int *gmax, int *err)
 {
     extern __shared__ uint32_t ctr32[];
     uint32_t *flag32 = ctr32 + kCountBytes / 4;
@@ -291,6 +334,7 @@ k_rows_fill(TailCtx tc, const int32_t *rowperm, const int32_t *rowflag, const in
     __shared__ int64_t ts[kMaxP], te[kMaxP];
     __shared__ int s_row, s_next;
     const int32_t n = tc.n, P = tc.P;
+    const int nr = *nrows;
     constexpr int32_t kCols = kCountBytes;
     int maxc = 0;
     // counters and flags start at zero; each compaction clears what it read
@@ -298,8 +342,8 @@ k_rows_fill(TailCtx tc, const int32_t *rowperm, const int32_t *rowflag, const in
         reinterpret_cast<uint4 *>(ctr32)[w] = make_uint4(0u, 0u, 0u, 0u);
     while (true) {
         const int qi = next_row(queue, &s_row);
-        if (qi >= n) break;
-        const int i = rowperm[qi];
+        if (qi >= nr) break;
+        const int i = rows[qi];
         if (rowflag[i]) continue;            // uniform across the block
         for (int p = threadIdx.x; p < P; p += blockDim.x) {
             int64_t s, e;
@@ -339,9 +383,10 @@ k_rows_fill(TailCtx tc, const int32_t *rowperm, const int32_t *rowflag, const in
 // rank < r* and the first `quota` rank-r* columns in column order.  A row
 // whose tail span fits one chunk keeps its pass-0 chunk for pass 1.
 __global__ void __launch_bounds__(kRowThreads)
-k_rows_capped(TailCtx tc, const int32_t *order, const int32_t *rowperm, const int32_t *rowflag,
-              const int64_t *cap_indptr, const int64_t *indptr, int32_t *indices, uint8_t *data,
-              int *queue, int *gmax, unsigned long long *disc, int *err)
+k_rows_capped(TailCtx tc, const int32_t *order, const int32_t *rows, const int *nrows,
+              const int32_t *rowflag, const int64_t *cap_indptr, const int64_t *indptr,
+              int32_t *indices, uint8_t *data, int *queue, int *gmax, unsigned long long *disc,
+              int *err)
 {
     extern __shared__ uint32_t sm[];
     uint32_t *ctr32 = sm;                      // kCapCols byte counters
@@ -351,12 +396,13 @@ k_rows_capped(TailCtx tc, const int32_t *order, const int32_t *rowperm, const in
     __shared__ int hist[kMaxP + 1];
     __shared__ int s_row, s_rstar, s_quota, s_seen, s_next;
     const int32_t n = tc.n, P = tc.P;
+    const int nr = *nrows;
     int maxc = 0;
     while (true) {
         const int qi = next_row(queue, &s_row);
-        if (qi >= n) break;
-        const int i = rowperm[qi];
-        if (!rowflag[i]) continue;
+        if (qi >= nr) break;
+        const int i = rows[qi];
+        if (!(rowflag[i] & 1)) continue;
         const int64_t cap = cap_indptr[i + 1] - cap_indptr[i];
         const bool one_chunk = (int64_t)n - ((int64_t)i + 1) <= kCapCols;
         for (int q = threadIdx.x; q <= P; q += blockDim.x) hist[q] = 0;
@@ -460,6 +506,407 @@ k_rows_capped(TailCtx tc, const int32_t *order, const int32_t *rowperm, const in
     if ((threadIdx.x & 31) == 0) atomicMax(gmax, maxc);
 }
 
+// ------------------------------------------------------------ pair tiles --
+// The second way to the same rows.  The rows are grouped by their cluster in
+// the row-order partition.  A group's neighbourhood N(g) is the sorted union
+// of every cluster (any partition) that holds one of its rows, cut to the
+// columns above the group's first row; every column that co-occurs with a
+// row of the group lies in it.  The count of a pair (i, j) is then a
+// comparison of the two label vectors: with the labels in FP16 (exact below
+// 2048; -1 and padding are NaN, which equals nothing) two partitions take one
+// HSET2 and one HADD2, and a 128 x 128 tile of pairs runs as a register-
+// blocked product with no atomics and no scattered loads.  A group takes the
+// tiles when their compare work (rows x |N(g)| x partition pairs) is at most
+// `ratio` times the member visits the streaming kernels would spend on its
+// rows; the others, and every row over its capacity, stay on the streaming
+// kernels.  Both ways produce the same counts, columns and order.
+
+__device__ __forceinline__ uint32_t label_half(int32_t l)
+{
+    return l >= 0 ? (uint32_t)__half_as_ushort(__int2half_rn(l)) : 0x7e00u;    // NaN
+}
+
+// lt[i*Q + w]: partitions (2w, 2w+1) of point i as a half2 (low half first)
+__global__ void k_labels_f16(const int32_t *labels, int32_t n, int32_t P, int32_t Q,
+                             uint32_t *lt)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        uint4 *dst = reinterpret_cast<uint4 *>(lt + i * Q);
+        for (int v = 0; v < Q / 4; ++v) {
+            uint32_t h[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int p = 8 * v + e;
+                h[e] = label_half(p < P ? labels[(int64_t)p * n + i] : -1);
+            }
+            dst[v] = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16),
+                                h[6] | (h[7] << 16));
+        }
+    }
+}
+
+struct GroupCtx {
+    const int32_t *labels, *members, *mypos;
+    const int64_t *S;
+    const int *prow;
+    int32_t n, P, K, Q;
+    int64_t ntiles;
+};
+
+// first position in members[a, b) whose point is above lo
+__device__ __forceinline__ int64_t first_above(const int32_t *members, int64_t a, int64_t b,
+                                               int32_t lo)
+{
+    while (a < b) {
+        const int64_t m = (a + b) >> 1;
+        if (members[m] > lo) b = m; else a = m + 1;
+    }
+    return a;
+}
+
+// One CTA per group (dynamic queue over the row-order partition's clusters):
+// the group's cluster lists, its rows' streaming cost, |N(g)| by chunked
+// bitmaps, the choice of path and, for the pair tiles, N(g) itself.
+__global__ void __launch_bounds__(kNbrThreads)
+k_nbr(GroupCtx gc, int64_t ratio, int32_t *nbr, int64_t nbr_cap, unsigned long long *nbr_used,
+      int64_t *grp_off, int32_t *grp_len, int32_t *grp_tiles, int32_t *rowflag, int *queue)
+{
+    extern __shared__ __align__(16) uint8_t nsm[];
+    uint32_t *bm = reinterpret_cast<uint32_t *>(nsm);
+    int64_t *ts = reinterpret_cast<int64_t *>(nsm + kNbrBytes);
+    int64_t *te = ts + kMaxGroupLists;
+    int32_t *cl = reinterpret_cast<int32_t *>(te + kMaxGroupLists);
+    __shared__ uint32_t lab[kDenseMaxK / 32];
+    __shared__ int s_g, s_nc, s_next, s_dense;
+    __shared__ int64_t s_off;
+    const int32_t n = gc.n, P = gc.P, K = gc.K;
+    const int64_t nt = gc.ntiles;
+    const int pr = *gc.prow;
+    constexpr int32_t kCols = kNbrBytes * 8;
+    for (;;) {
+        const int g = next_row(queue, &s_g);
+        if (g >= K) break;
+        const int64_t gb = gc.S[((int64_t)pr * K + g) * nt];
+        const int64_t size = gc.S[((int64_t)pr * K + g + 1) * nt] - gb;
+        if (size == 0) {
+            if (threadIdx.x == 0) grp_tiles[g] = 0;
+            continue;
+        }
+        const int32_t *rows = gc.members + gb;
+        const int32_t lo = rows[0];
+        // 1. the clusters holding the group's rows, partition by partition
+        if (threadIdx.x == 0) s_nc = 0;
+        int64_t visits = 0;
+        for (int p = 0; p < P; ++p) {
+            for (int w = threadIdx.x; w < (K + 31) / 32; w += blockDim.x) lab[w] = 0u;
+            __syncthreads();
+            for (int64_t t = threadIdx.x; t < size; t += blockDim.x) {
+                const int32_t i = rows[t];
+                const int32_t c = gc.labels[(int64_t)p * n + i];
+                if (c >= 0 && c < K) {
+                    atomicOr(&lab[c >> 5], 1u << (c & 31));
+                    visits += gc.S[((int64_t)p * K + c + 1) * nt] -
+                              gc.mypos[(int64_t)p * n + i] - 1;
+                }
+            }
+            __syncthreads();
+            for (int w = threadIdx.x; w < (K + 31) / 32; w += blockDim.x)
+                for (uint32_t b = lab[w]; b; b &= b - 1u) {
+                    const int slot = atomicAdd(&s_nc, 1);
+                    if (slot < kMaxGroupLists) cl[slot] = p * K + w * 32 + __ffs(b) - 1;
+                }
+            __syncthreads();
+        }
+        visits = block_sum<kNbrThreads>(visits);
+        const int nc = s_nc;
+        bool dense = nc <= kMaxGroupLists;
+        int64_t total = 0;
+        for (int pass = 0; pass < 2 && dense; ++pass) {
+            // cursors: each list from its first member above the group's first row
+            for (int e = threadIdx.x; e < nc; e += blockDim.x) {
+                const int64_t a = gc.S[(int64_t)cl[e] * nt], b = gc.S[((int64_t)cl[e] + 1) * nt];
+                ts[e] = first_above(gc.members, a, b, lo);
+                te[e] = b;
+            }
+            __syncthreads();
+            int64_t at = 0;
+            for (int64_t j0 = (int64_t)lo + 1; j0 < n; j0 += kCols) {
+                const int32_t jl = (int32_t)((j0 + kCols < n) ? j0 + kCols : n);
+                const int nvec = (int)((jl - j0 + 127) >> 7);
+                uint4 *b4 = reinterpret_cast<uint4 *>(bm);
+                for (int v = threadIdx.x; v < nvec; v += blockDim.x) b4[v] = make_uint4(0u, 0u, 0u, 0u);
+                if (threadIdx.x == 0) s_next = 0;
+                __syncthreads();
+                const int32_t jb = (int32_t)j0;
+                stream_chunk(gc.members, ts, te, nc, jl, &s_next, [&](int32_t j, int) {
+                    const int32_t o = j - jb;
+                    atomicOr(&bm[o >> 5], 1u << (o & 31));
+                });
+                __syncthreads();
+                // each thread owns a run of vectors; pass 1 writes its columns in order
+                const int per = (nvec + kNbrThreads - 1) / kNbrThreads;
+                const int v0 = min(nvec, (int)threadIdx.x * per), v1 = min(nvec, v0 + per);
+                int64_t c = 0;
+                for (int v = v0; v < v1; ++v) {
+                    const uint4 x = b4[v];
+                    c += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+                }
+                int64_t tot;
+                const int64_t pre = block_excl_sum_shfl<kNbrThreads>(c, tot);
+                if (pass == 1) {
+                    int32_t *out = nbr + s_off + at + pre;
+                    for (int v = v0; v < v1; ++v)
+                        for (int q = 0; q < 4; ++q)
+                            for (uint32_t b = bm[4 * v + q]; b; b &= b - 1u)
+                                *out++ = jb + 128 * v + 32 * q + __ffs(b) - 1;
+                }
+                at += tot;
+                __syncthreads();
+            }
+            if (pass == 1) break;
+            total = at;
+            // the choice: the tiles' compare work against the streaming visits
+            int64_t est = 0;
+            const double span = (double)max(1, n - 1 - lo);
+            for (int64_t t = threadIdx.x; t * kPT < size; t += blockDim.x)
+                est += (int64_t)((double)kPT * gc.Q * (double)total *
+                                 ((double)(n - 1 - rows[t * kPT]) / span));
+            est = block_sum<kNbrThreads>(est);
+            if (threadIdx.x == 0) {
+                int d = ratio > 0 && est <= ratio * visits;
+                if (d) {
+                    const unsigned long long o = atomicAdd(nbr_used, (unsigned long long)total);
+                    d = (int64_t)(o + total) <= nbr_cap;
+                    s_off = (int64_t)o;
+                }
+                s_dense = d;
+            }
+            __syncthreads();
+            dense = s_dense;
+        }
+        if (threadIdx.x == 0) {
+            grp_tiles[g] = dense ? (int32_t)((size + kPT - 1) / kPT) : 0;
+            grp_off[g] = dense ? s_off : 0;
+            grp_len[g] = dense ? (int32_t)total : 0;
+        }
+        if (dense)
+            for (int64_t t = threadIdx.x; t < size; t += blockDim.x) rowflag[rows[t]] = 2;
+        __syncthreads();
+    }
+}
+
+struct PairCtx {
+    const uint32_t *lt;
+    const int32_t *members, *nbr;
+    const int64_t *S, *grp_off, *item0;
+    const int32_t *grp_len;
+    const int *prow;
+    int32_t n, K, Q;
+    int64_t ntiles;
+};
+
+// 128 points' label pairs into s[w*128 + r] (-1: a NaN column)
+__device__ __forceinline__ void load_pairs(uint32_t *s, const int32_t *idx, const uint32_t *lt,
+                                           int32_t Q)
+{
+    for (int k = threadIdx.x; k < kPT * (Q / 4); k += blockDim.x) {
+        const int r = k & (kPT - 1), v = k >> 7;
+        const int32_t i = idx[r];
+        const uint4 x = i >= 0 ? *reinterpret_cast<const uint4 *>(lt + (int64_t)i * Q + 4 * v)
+                               : make_uint4(0x7e007e00u, 0x7e007e00u, 0x7e007e00u, 0x7e007e00u);
+        s[(4 * v) * kPT + r] = x.x;
+        s[(4 * v + 1) * kPT + r] = x.y;
+        s[(4 * v + 2) * kPT + r] = x.z;
+        s[(4 * v + 3) * kPT + r] = x.w;
+    }
+}
+
+// One CTA per (group, 128-row block), from a queue over all groups' blocks.
+// Thread (tx, ty) of a 16 x 16 grid owns rows 8ty..8ty+7 and columns
+// 8tx..8tx+7 of each tile; a row's columns are spread over one half-warp, in
+// column order, so its kept entries are placed with a 16-lane prefix sum.
+// COUNT: distinct columns per row -> rowcnt, rowflag (and the first
+// partition's overflow check).  FILL: the kept entries at indptr[i].
+template <bool FILL>
+__global__ void __launch_bounds__(kPairThreads, 2)
+k_pairs(PairCtx pc, TailCtx tc, const int32_t *order, const int64_t *cap_indptr,
+        const int64_t *indptr, int32_t *rowcnt, int32_t *rowflag, int32_t *indices,
+        uint8_t *data, int *queue, int *gmax, int *err)
+{
+    extern __shared__ __align__(16) uint32_t psm[];
+    const int32_t Q = pc.Q, K = pc.K;
+    uint32_t *sR = psm;
+    uint32_t *sC = psm + (size_t)Q * kPT;
+    __shared__ int32_t s_row[kPT], s_col[kPT];
+    __shared__ int64_t s_end[kPT];
+    __shared__ int s_item, s_c0;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int pr = *pc.prow;
+    const int64_t nitems = pc.item0[K];
+    int maxc = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(queue, 1);
+        __syncthreads();
+        const int64_t t = s_item;
+        if (t >= nitems) break;
+        int glo = 0, ghi = K;                       // item0[glo] <= t < item0[ghi]
+        while (ghi - glo > 1) {
+            const int m = (glo + ghi) >> 1;
+            if (pc.item0[m] <= t) glo = m; else ghi = m;
+        }
+        const int g = glo;
+        const int64_t gb = pc.S[((int64_t)pr * K + g) * pc.ntiles];
+        const int64_t size = pc.S[((int64_t)pr * K + g + 1) * pc.ntiles] - gb;
+        const int64_t r0 = (t - pc.item0[g]) * kPT;
+        const int nrow = (int)(size - r0 < kPT ? size - r0 : kPT);
+        for (int r = threadIdx.x; r < kPT; r += blockDim.x) {
+            const int32_t i = r < nrow ? pc.members[gb + r0 + r] : -1;
+            s_row[r] = i;
+            if (FILL) s_end[r] = i >= 0 ? indptr[i + 1] : 0;
+        }
+        __syncthreads();
+        load_pairs(sR, s_row, pc.lt, Q);
+        const int32_t *nb = pc.nbr + pc.grp_off[g];
+        const int32_t len = pc.grp_len[g];
+        if (threadIdx.x == 0) {
+            int a = 0, b = len;
+            const int32_t first = s_row[0];
+            while (a < b) {
+                const int m = (a + b) >> 1;
+                if (nb[m] > first) b = m; else a = m + 1;
+            }
+            s_c0 = a;
+        }
+        // this thread's rows: a row that takes no entries compares as INT_MAX
+        int32_t ri[8];
+        int64_t cur[8];
+        int dcount[8];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const int32_t i = s_row[8 * ty + a];
+            bool live = i >= 0;
+            if (FILL && live) live = !(rowflag[i] & 1);
+            ri[a] = live ? i : 0x7fffffff;
+            cur[a] = (FILL && live) ? indptr[i] : 0;
+            dcount[a] = 0;
+        }
+        __syncthreads();
+        for (int cb = s_c0; cb < len; cb += kPT) {
+            for (int c = threadIdx.x; c < kPT; c += blockDim.x)
+                s_col[c] = cb + c < len ? nb[cb + c] : -1;
+            __syncthreads();
+            load_pairs(sC, s_col, pc.lt, Q);
+            __syncthreads();
+            __half2 acc[8][8];
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+                for (int b = 0; b < 8; ++b) acc[a][b] = __float2half2_rn(0.f);
+#pragma unroll 2
+            for (int w = 0; w < Q; ++w) {
+                const uint4 ra = *reinterpret_cast<const uint4 *>(sR + w * kPT + 8 * ty);
+                const uint4 rb = *reinterpret_cast<const uint4 *>(sR + w * kPT + 8 * ty + 4);
+                const uint4 ca = *reinterpret_cast<const uint4 *>(sC + w * kPT + 8 * tx);
+                const uint4 cc = *reinterpret_cast<const uint4 *>(sC + w * kPT + 8 * tx + 4);
+                const uint32_t R[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
+                const uint32_t C[8] = {ca.x, ca.y, ca.z, ca.w, cc.x, cc.y, cc.z, cc.w};
+#pragma unroll
+                for (int a = 0; a < 8; ++a) {
+                    const __half2 rv = *reinterpret_cast<const __half2 *>(&R[a]);
+#pragma unroll
+                    for (int b = 0; b < 8; ++b)
+                        acc[a][b] = __hadd2(acc[a][b],
+                                            __heq2(rv, *reinterpret_cast<const __half2 *>(&C[b])));
+                }
+            }
+            int32_t cj[8];
+#pragma unroll
+            for (int b = 0; b < 8; ++b) cj[b] = s_col[8 * tx + b];
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                uint32_t keep = 0;
+                int cnt[8];
+#pragma unroll
+                for (int b = 0; b < 8; ++b) {
+                    cnt[b] = (int)(__low2float(acc[a][b]) + __high2float(acc[a][b]));
+                    if (cj[b] > ri[a] && cnt[b] > 0) keep |= 1u << b;
+                }
+                const int k = __popc(keep);
+                if (FILL) {
+                    int incl = k;
+#pragma unroll
+                    for (int d = 1; d < 16; d <<= 1) {
+                        const int v = __shfl_up_sync(0xffffffffu, incl, d, 16);
+                        if (tx >= d) incl += v;
+                    }
+                    const int tot = __shfl_sync(0xffffffffu, incl, 15, 16);
+                    int64_t at = cur[a] + incl - k;
+                    const int64_t end = s_end[8 * ty + a];
+#pragma unroll
+                    for (int b = 0; b < 8; ++b)
+                        if ((keep & (1u << b)) && at < end) {
+                            indices[at] = cj[b];
+                            data[at] = (uint8_t)cnt[b];
+                            maxc = max(maxc, cnt[b]);
+                            ++at;
+                        }
+                    cur[a] += tot;
+                } else {
+                    dcount[a] += k;
+                }
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const int32_t i = s_row[8 * ty + a];
+            if (FILL) {
+                if (tx == 0 && ri[a] != 0x7fffffff && cur[a] != indptr[i + 1])
+                    set_err(err, DEV_CAPACITY);
+            } else {
+                int d = dcount[a];
+#pragma unroll
+                for (int o = 8; o >= 1; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o, 16);
+                if (tx == 0 && i >= 0) {
+                    const int64_t cap = cap_indptr[i + 1] - cap_indptr[i];
+                    rowcnt[i] = (int32_t)(d < cap ? d : cap);
+                    rowflag[i] = 2 | (d > cap ? 1 : 0);
+                    // the first partition in processing order takes no capacity check
+                    int64_t s, e;
+                    tc.tail(i, order[0], s, e);
+                    if (e - s > cap) set_err(err, DEV_FIRST_OVERFLOW);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (FILL) {
+        for (int d = 16; d >= 1; d >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, d));
+        if ((threadIdx.x & 31) == 0) atomicMax(gmax, maxc);
+    }
+}
+
+// rows of the row order whose flag bits under `mask` equal `want`, kept in
+// that order within each warp's 32 (the lists the streaming kernels take)
+__global__ void k_pick_rows(const int32_t *rowperm, int32_t n, const int32_t *rowflag, int mask,
+                            int want, int32_t *out, int *count)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~(int64_t)31; b < n;
+         b += stride) {
+        const int64_t q = b + lane;
+        const int32_t i = q < n ? rowperm[q] : -1;
+        const bool sel = i >= 0 && (rowflag[i] & mask) == want;
+        const unsigned m = __ballot_sync(0xffffffffu, sel);
+        int base = 0;
+        if (lane == 0 && m) base = atomicAdd(count, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (sel) out[base + __popc(m & ((1u << lane) - 1u))] = i;
+    }
+}
+
 __global__ void k_diassoc_val(uint8_t *data, int64_t nnz, uint32_t top)
 {
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz;
@@ -482,11 +929,12 @@ __global__ void k_diassoc(uint8_t *data, int64_t nnz, const int *gmax)
 // points -- and read them from L2 instead of HBM.
 __global__ void k_rowperm(const int32_t *labels, int32_t n, int32_t P, int32_t K, int64_t ntiles,
                           const int32_t *members, const int64_t *S, const int32_t *ncl,
-                          int32_t *rowperm, int *counter)
+                          int32_t *rowperm, int *counter, int *prow)
 {
     int pr = 0;
     for (int p = 1; p < P; ++p)
         if (ncl[p] > ncl[pr]) pr = p;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *prow = pr;
     const int64_t s0 = S[(int64_t)pr * K * ntiles], s1 = S[((int64_t)pr + 1) * K * ntiles];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < s1 - s0; q += stride)
@@ -520,6 +968,22 @@ static int row_grid(int ctas_per_sm = 2)
     return ctas_per_sm * sms;
 }
 
+template <bool FILL>
+static int launch_pairs(const CoWS &w, const TailCtx &tc, const int64_t *cap_indptr,
+                        const int64_t *indptr, int32_t *indices, uint8_t *data, cudaStream_t st)
+{
+    const size_t smem = (size_t)2 * w.Q * kPT * sizeof(uint32_t);
+    if (smem > 200 * 1024) return EACB_ERR_UNSUPPORTED;
+    EACB_CUDA(allow_max_dyn_smem(k_pairs<FILL>));
+    PairCtx pc{w.lt, w.members, w.nbr, w.S, w.grp_off, w.grp_item0, w.grp_len, w.prow,
+               tc.n, tc.K, w.Q, w.ntiles};
+    k_pairs<FILL><<<row_grid(2), kPairThreads, smem, st>>>(
+        pc, tc, w.order, cap_indptr, indptr, w.rowcnt, w.rowflag, indices, data,
+        &w.queue[FILL ? 6 : 5], w.maxcnt, w.err);
+    EACB_CHECK_LAUNCH();
+    return EACB_OK;
+}
+
 }  // namespace eacb
 
 using namespace eacb;
@@ -543,7 +1007,7 @@ extern "C" int eacb_coassoc_prepare(const int32_t *labels, int32_t n, int32_t P,
     CoWS w = CoWS::carve(c, n, P, K);
     if (c.overflow) return EACB_ERR_WORKSPACE;
     EACB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(int), st));
-    EACB_CUDA(cudaMemsetAsync(w.queue, 0, 4 * sizeof(int), st));
+    EACB_CUDA(cudaMemsetAsync(w.queue, 0, kQueues * sizeof(int), st));
     const int64_t nt = w.ntiles;
     const int64_t m = (int64_t)P * K * nt;
     k_ml_count<<<(unsigned)(P * nt), 256, K * sizeof(int), st>>>(labels, n, K, nt, w.cnt, w.err);
@@ -561,8 +1025,26 @@ extern "C" int eacb_coassoc_prepare(const int32_t *labels, int32_t n, int32_t P,
     k_order<<<1, 32, 0, st>>>(w.ncl, P, w.order);
     EACB_CHECK_LAUNCH();
     k_rowperm<<<grid_for(n, 256), 256, 0, st>>>(labels, n, P, K, nt, w.members, w.S, w.ncl,
-                                                 w.rowperm, &w.queue[3]);
+                                                 w.rowperm, &w.queue[3], w.prow);
     EACB_CHECK_LAUNCH();
+    // the path of each group (pair tiles or streaming) and the neighbourhoods
+    EACB_CUDA(cudaMemsetAsync(w.rowflag, 0, sizeof(int32_t) * n, st));
+    EACB_CUDA(cudaMemsetAsync(w.grp_tiles, 0, sizeof(int32_t) * ((size_t)K + 1), st));
+    const int64_t ratio = K <= kDenseMaxK ? tune_get(TUNE_CO_DENSE, P, n, kDenseRatioDefault) : 0;
+    if (ratio > 0) {
+        k_labels_f16<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(labels, n, P, w.Q, w.lt);
+        EACB_CHECK_LAUNCH();
+        EACB_CUDA(cudaMemsetAsync(w.nbr_used, 0, sizeof(unsigned long long), st));
+        EACB_CUDA(allow_max_dyn_smem(k_nbr));
+        GroupCtx gc{labels, w.members, w.mypos, w.S, w.prow, n, P, K, w.Q, nt};
+        k_nbr<<<row_grid(1), kNbrThreads, kNbrSmem, st>>>(gc, ratio, w.nbr, w.nbr_cap, w.nbr_used,
+                                                          w.grp_off, w.grp_len, w.grp_tiles,
+                                                          w.rowflag, &w.queue[4]);
+        EACB_CHECK_LAUNCH();
+    }
+    if ((s = scan_launch<int32_t, int64_t>(w.grp_tiles, w.grp_item0, K, 0, &w.grp_item0[K],
+                                           w.scan, st)))
+        return s;
     int mc = 0;
     EACB_CUDA(cudaMemcpyAsync(&mc, w.maxcnt, sizeof(int), cudaMemcpyDeviceToHost, st));
     if ((s = read_err(w.err, st))) return s;
@@ -581,13 +1063,19 @@ extern "C" int eacb_coassoc_count(const int32_t *labels, int32_t n, int32_t P, i
     Carver c(ws, ws_bytes);
     CoWS w = CoWS::carve(c, n, P, K);
     if (c.overflow) return EACB_ERR_WORKSPACE;
-    EACB_CUDA(cudaMemsetAsync(w.queue, 0, 4 * sizeof(int), st));
+    EACB_CUDA(cudaMemsetAsync(w.queue, 0, kQueues * sizeof(int), st));
     TailCtx tc{labels, w.members, w.mypos, w.S, n, P, K, w.ntiles};
     EACB_CUDA(allow_max_dyn_smem(k_rows_count));
     ProfScope ps(PROF_COASSOC, st);
+    if ((s = launch_pairs<false>(w, tc, cap_indptr, nullptr, nullptr, nullptr, st))) return s;
+    // the streamed rows: those outside the pair tiles' groups
+    EACB_CUDA(cudaMemsetAsync(w.rowlist_n, 0, sizeof(int), st));
+    k_pick_rows<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(w.rowperm, n, w.rowflag, 2, 0,
+                                                           w.rowlist, w.rowlist_n);
+    EACB_CHECK_LAUNCH();
     k_rows_count<<<row_grid((int)tune_get(TUNE_CO_COUNT_CTAS, P, n, 2)), kRowThreads, kBitmapBytes,
                    st>>>(
-        tc, w.order, w.rowperm, cap_indptr, w.rowcnt, w.rowflag, &w.queue[0], w.err);
+        tc, w.order, w.rowlist, w.rowlist_n, cap_indptr, w.rowcnt, w.rowflag, &w.queue[0], w.err);
     EACB_CHECK_LAUNCH();
     ps.done(0.0);
     if ((s = scan_launch<int32_t, int64_t>(w.rowcnt, indptr, n, 0, &indptr[n], w.scan, st))) return s;
@@ -678,21 +1166,32 @@ extern "C" int eacb_coassoc_fill(const int32_t *labels, int32_t n, int32_t P, in
     Carver c(ws, ws_bytes);
     CoWS w = CoWS::carve(c, n, P, K);
     if (c.overflow) return EACB_ERR_WORKSPACE;
-    EACB_CUDA(cudaMemsetAsync(w.queue, 0, 4 * sizeof(int), st));
+    EACB_CUDA(cudaMemsetAsync(w.queue, 0, kQueues * sizeof(int), st));
     EACB_CUDA(cudaMemsetAsync(w.disc, 0, sizeof(unsigned long long), st));
     EACB_CUDA(cudaMemsetAsync(w.maxcnt, 0, sizeof(int), st));
     TailCtx tc{labels, w.members, w.mypos, w.S, n, P, K, w.ntiles};
     EACB_CUDA(allow_max_dyn_smem(k_rows_fill));
     EACB_CUDA(allow_max_dyn_smem(k_rows_capped));
     ProfScope ps(PROF_COASSOC, st);
+    if ((s = launch_pairs<true>(w, tc, cap_indptr, indptr, indices, data, st))) return s;
+    EACB_CUDA(cudaMemsetAsync(w.rowlist_n, 0, sizeof(int), st));
+    k_pick_rows<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(w.rowperm, n, w.rowflag, 3, 0,
+                                                           w.rowlist, w.rowlist_n);
+    EACB_CHECK_LAUNCH();
     k_rows_fill<<<row_grid((int)tune_get(TUNE_CO_FILL_CTAS, P, n, 2)), kFillThreads, kFillSmem,
                   st>>>(
-        tc, w.rowperm, w.rowflag, indptr, indices, data, &w.queue[1], w.maxcnt, w.err);
+        tc, w.rowlist, w.rowlist_n, w.rowflag, indptr, indices, data, &w.queue[1], w.maxcnt,
+        w.err);
     EACB_CHECK_LAUNCH();
     ps.done(0.0);
+    // rows over their capacity, from either path
+    EACB_CUDA(cudaMemsetAsync(w.rowlist_n, 0, sizeof(int), st));
+    k_pick_rows<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(w.rowperm, n, w.rowflag, 1, 1,
+                                                           w.rowlist, w.rowlist_n);
+    EACB_CHECK_LAUNCH();
     k_rows_capped<<<row_grid(), kRowThreads, kCapSmem, st>>>(
-        tc, w.order, w.rowperm, w.rowflag, cap_indptr, indptr, indices, data, &w.queue[2],
-        w.maxcnt, w.disc, w.err);
+        tc, w.order, w.rowlist, w.rowlist_n, w.rowflag, cap_indptr, indptr, indices, data,
+        &w.queue[2], w.maxcnt, w.disc, w.err);
     EACB_CHECK_LAUNCH();
     int64_t nnz = 0;
     EACB_CUDA(cudaMemcpyAsync(&nnz, &indptr[n], sizeof(int64_t), cudaMemcpyDeviceToHost, st));

@@ -31,7 +31,9 @@ enum TuneKnob : int {
     TUNE_CO_FILL_CTAS = 3,     // co-association fill pass CTAs per SM; a = P, b = n
     TUNE_MST_PHASE1 = 4,       // graph MST: first phase's share of the entries, per mille; a = 0, b = V
     TUNE_ROUND_TEAM = 5,       // Boruvka round kernel participants at most; a = 0 graph, 1 EAC; b = V
-    TUNE_NKNOBS = 6
+    TUNE_CO_DENSE = 6,         // co-association pair tiles: compare work allowed per streamed
+                               // member visit (0: streaming only); a = P, b = n
+    TUNE_NKNOBS = 7
 };
 int64_t tune_get(int knob, int64_t a, int64_t b, int64_t dflt);
 }

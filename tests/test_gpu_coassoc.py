@@ -88,6 +88,85 @@ def test_coassoc_vs_oracle(T, seed, n, P, kmin, kmax, factor, kind, holes):
     assert np.array_equal(c.data.cpu().numpy(), cnt)
 
 
+def _clustered_labels(rng, P, n, groups, split, holes=0.0):
+    """Labels with the structure of an EAC ensemble: every partition splits
+    each of `groups` point groups into a few clusters of its own."""
+    g = rng.integers(0, groups, n)
+    L = np.empty((P, n), dtype=np.int32)
+    for p in range(P):
+        s = int(rng.integers(split[0], split[1] + 1))
+        L[p] = g * s + rng.integers(0, s, n)
+        if holes:
+            L[p][rng.random(n) < holes] = -1
+    return L
+
+
+PATH_CASES = [
+    # labels, seed, n, P, (k range | groups, split range), factor, capacity, holes
+    ("random", 1, 3000, 20, (5, 40), 3, "linear", 0.0),
+    ("random", 2, 5000, 37, (2, 9), 1, "linear", 0.0),          # discards: capped rows
+    ("random", 3, 4000, 12, (30, 300), 2, "constant", 0.05),    # -1 labels
+    ("random", 5, 2500, 255, (10, 20), 3, "linear", 0.0),       # 255 partitions
+    ("clustered", 7, 20000, 50, (40, 3, 6), 3, "linear", 0.0),  # EAC-like structure
+    ("clustered", 8, 8000, 100, (12, 2, 5), 1, "linear", 0.02),  # discards and holes
+    ("clustered", 9, 550_000, 2, (500, 1, 4), 3, "linear", 0.0),  # neighbourhoods over chunks
+]
+_PATH_REF = {}
+
+
+def _path_case(case):
+    kind_l, seed, n, P, shape, factor, kind, holes = case
+    if case not in _PATH_REF:
+        rng = np.random.default_rng(seed)
+        if kind_l == "random":
+            L = _random_labels(rng, P, n, shape[0], shape[1], holes)
+        else:
+            L = _clustered_labels(rng, P, n, shape[0], shape[1:], holes)
+        ma = oracle.max_cluster_size(L) * factor
+        cap = oracle.indptr_linear(n, ma) if kind == "linear" else oracle.indptr_constant(n, ma)
+        _PATH_REF.clear()
+        _PATH_REF[case] = (L, ma, oracle.coassoc_build(L, cap))
+    return _PATH_REF[case]
+
+
+@pytest.mark.parametrize("ratio", [0, 10 ** 9])
+@pytest.mark.parametrize("case", PATH_CASES, ids=[f"{c[0]}{c[1]}" for c in PATH_CASES])
+def test_coassoc_paths_vs_oracle(T, case, ratio):
+    """The same build with every group forced onto the streaming kernels
+    (ratio 0) and onto the pair tiles (ratio 1e9; capped rows still stream)
+    equals the oracle."""
+    from masters_final_b200 import _lib
+    L, ma, (ip, ind, cnt, nnz, disc, st) = _path_case(case)
+    assert st == 0
+    with _lib.forced("co_dense_ratio", ratio):
+        c = _build(L, case[2], ma, case[6])
+    assert c.nnz == nnz and c.nnz_discarded == disc
+    assert np.array_equal(c.indptr.cpu().numpy(), ip)
+    assert np.array_equal(c.indices.cpu().numpy(), ind)
+    assert np.array_equal(c.data.cpu().numpy(), cnt)
+
+
+@pytest.mark.parametrize("name", ["eac_small", "eac_discard", "eac_10k"])
+def test_coassoc_golden_pair_tiles(T, name):
+    """The reference-run fixtures with every group on the pair tiles."""
+    from masters_final_b200 import _lib
+    g = golden(name)
+    n = g["x"].shape[0]
+    with _lib.forced("co_dense_ratio", 10 ** 9):
+        c = _build(g["labels_matrix"].astype(np.int32), n, g["max_assocs"])
+    assert c.nnz == g["nnz"] and c.nnz_discarded == g["nnz_discarded"]
+    c.make_diassoc()
+    if name == "eac_10k":
+        h = hashlib.sha256()
+        for arr in (c.indptr.cpu().numpy(), c.indices.cpu().numpy(), c.data.cpu().numpy()):
+            h.update(np.ascontiguousarray(arr).tobytes())
+        assert h.hexdigest() == str(g["coassoc_sha"])
+    else:
+        assert np.array_equal(c.indptr.cpu().numpy(), g["indptr"])
+        assert np.array_equal(c.indices.cpu().numpy(), g["indices"])
+        assert np.array_equal(c.data.cpu().numpy(), g["diassoc"])
+
+
 def test_first_partition_overflow_raises(T):
     from masters_final_b200.EAC.sparse import EAC_CSR
     n = 1000
