@@ -706,7 +706,14 @@ struct PairCtx {
     int64_t ntiles;
 };
 
-// 128 points' label pairs into s[w*128 + r] (-1: a NaN column)
+// Column c of a tile sits at slot 8 (c % 16) + c / 16, so that the eight
+// slots 8tx..8tx+7 a thread reads with two 16-byte loads are the columns
+// tx, tx + 16, ..., tx + 112: each group of 16 consecutive columns is then
+// held by the 16 lanes of a half-warp, one column per lane.
+__device__ __forceinline__ int col_slot(int c) { return ((c & 15) << 3) | (c >> 4); }
+
+// 128 points' label pairs into s[w*128 + slot] (-1: a NaN point); idx is
+// indexed by slot
 __device__ __forceinline__ void load_pairs(uint32_t *s, const int32_t *idx, const uint32_t *lt,
                                            int32_t Q)
 {
@@ -723,9 +730,10 @@ __device__ __forceinline__ void load_pairs(uint32_t *s, const int32_t *idx, cons
 }
 
 // One CTA per (group, 128-row block), from a queue over all groups' blocks.
-// Thread (tx, ty) of a 16 x 16 grid owns rows 8ty..8ty+7 and columns
-// 8tx..8tx+7 of each tile; a row's columns are spread over one half-warp, in
-// column order, so its kept entries are placed with a 16-lane prefix sum.
+// Thread (tx, ty) of a 16 x 16 grid owns rows 8ty..8ty+7 and columns tx +
+// 16b (b = 0..7) of each tile.  A row's 16 consecutive columns 16b..16b+15
+// are then one per lane of a half-warp: a ballot places its kept entries, and
+// the half-warp writes them to consecutive positions with one store.
 // COUNT: distinct columns per row -> rowcnt, rowflag (and the first
 // partition's overflow check).  FILL: the kept entries at indptr[i].
 template <bool FILL>
@@ -739,7 +747,7 @@ k_pairs(PairCtx pc, TailCtx tc, const int32_t *order, const int64_t *cap_indptr,
     uint32_t *sR = psm;
     uint32_t *sC = psm + (size_t)Q * kPT;
     __shared__ int32_t s_row[kPT], s_col[kPT];
-    __shared__ int64_t s_end[kPT];
+    __shared__ int64_t s_end[kPT], s_cur[kPT];
     __shared__ int s_item, s_c0;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int pr = *pc.prow;
@@ -763,7 +771,10 @@ k_pairs(PairCtx pc, TailCtx tc, const int32_t *order, const int64_t *cap_indptr,
         for (int r = threadIdx.x; r < kPT; r += blockDim.x) {
             const int32_t i = r < nrow ? pc.members[gb + r0 + r] : -1;
             s_row[r] = i;
-            if (FILL) s_end[r] = i >= 0 ? indptr[i + 1] : 0;
+            if (FILL) {
+                s_end[r] = i >= 0 ? indptr[i + 1] : 0;
+                s_cur[r] = i >= 0 ? indptr[i] : 0;
+            }
         }
         __syncthreads();
         load_pairs(sR, s_row, pc.lt, Q);
@@ -780,7 +791,6 @@ k_pairs(PairCtx pc, TailCtx tc, const int32_t *order, const int64_t *cap_indptr,
         }
         // this thread's rows: a row that takes no entries compares as INT_MAX
         int32_t ri[8];
-        int64_t cur[8];
         int dcount[8];
 #pragma unroll
         for (int a = 0; a < 8; ++a) {
@@ -788,13 +798,12 @@ k_pairs(PairCtx pc, TailCtx tc, const int32_t *order, const int64_t *cap_indptr,
             bool live = i >= 0;
             if (FILL && live) live = !(rowflag[i] & 1);
             ri[a] = live ? i : 0x7fffffff;
-            cur[a] = (FILL && live) ? indptr[i] : 0;
             dcount[a] = 0;
         }
         __syncthreads();
         for (int cb = s_c0; cb < len; cb += kPT) {
             for (int c = threadIdx.x; c < kPT; c += blockDim.x)
-                s_col[c] = cb + c < len ? nb[cb + c] : -1;
+                s_col[col_slot(c)] = cb + c < len ? nb[cb + c] : -1;
             __syncthreads();
             load_pairs(sC, s_col, pc.lt, Q);
             __syncthreads();
@@ -823,37 +832,34 @@ k_pairs(PairCtx pc, TailCtx tc, const int32_t *order, const int64_t *cap_indptr,
             int32_t cj[8];
 #pragma unroll
             for (int b = 0; b < 8; ++b) cj[b] = s_col[8 * tx + b];
+            const int half = threadIdx.x & 16;              // this half-warp's ballot bits
+            const uint32_t below = (1u << tx) - 1u;
 #pragma unroll
             for (int a = 0; a < 8; ++a) {
-                uint32_t keep = 0;
-                int cnt[8];
+                // the half-warp's lanes all read the cursor before the first
+                // ballot and lane 0 advances it after the last
+                int64_t at = FILL ? s_cur[8 * ty + a] : 0;
+                const int64_t end = FILL ? s_end[8 * ty + a] : 0;
 #pragma unroll
                 for (int b = 0; b < 8; ++b) {
-                    cnt[b] = (int)(__low2float(acc[a][b]) + __high2float(acc[a][b]));
-                    if (cj[b] > ri[a] && cnt[b] > 0) keep |= 1u << b;
-                }
-                const int k = __popc(keep);
-                if (FILL) {
-                    int incl = k;
-#pragma unroll
-                    for (int d = 1; d < 16; d <<= 1) {
-                        const int v = __shfl_up_sync(0xffffffffu, incl, d, 16);
-                        if (tx >= d) incl += v;
-                    }
-                    const int tot = __shfl_sync(0xffffffffu, incl, 15, 16);
-                    int64_t at = cur[a] + incl - k;
-                    const int64_t end = s_end[8 * ty + a];
-#pragma unroll
-                    for (int b = 0; b < 8; ++b)
-                        if ((keep & (1u << b)) && at < end) {
-                            indices[at] = cj[b];
-                            data[at] = (uint8_t)cnt[b];
-                            maxc = max(maxc, cnt[b]);
-                            ++at;
+                    const int cnt = (int)(__low2float(acc[a][b]) + __high2float(acc[a][b]));
+                    const bool keep = cj[b] > ri[a] && cnt > 0;
+                    if (FILL) {
+                        const uint32_t m = (__ballot_sync(0xffffffffu, keep) >> half) & 0xffffu;
+                        const int64_t pos = at + __popc(m & below);
+                        if (keep && pos < end) {
+                            indices[pos] = cj[b];
+                            data[pos] = (uint8_t)cnt;
+                            maxc = max(maxc, cnt);
                         }
-                    cur[a] += tot;
-                } else {
-                    dcount[a] += k;
+                        at += __popc(m);
+                    } else {
+                        dcount[a] += keep;
+                    }
+                }
+                if (FILL) {
+                    __syncwarp();
+                    if (tx == 0) s_cur[8 * ty + a] = at;
                 }
             }
             __syncthreads();
@@ -862,7 +868,7 @@ k_pairs(PairCtx pc, TailCtx tc, const int32_t *order, const int64_t *cap_indptr,
         for (int a = 0; a < 8; ++a) {
             const int32_t i = s_row[8 * ty + a];
             if (FILL) {
-                if (tx == 0 && ri[a] != 0x7fffffff && cur[a] != indptr[i + 1])
+                if (tx == 0 && ri[a] != 0x7fffffff && s_cur[8 * ty + a] != indptr[i + 1])
                     set_err(err, DEV_CAPACITY);
             } else {
                 int d = dcount[a];
