@@ -828,6 +828,24 @@ def case_label_tc_100k():
     return {"ks": ks, "iters": out[3].tolist()}
 
 
+def case_ensemble_500k_20p():
+    """K-Means ensemble of the 500,000-point workload's data (16-D, 50
+    anisotropic Gaussians) with 20 of its 200 partitions (k in [350, 711),
+    3 Lloyd iterations, BF16 labeler): every kernel of the ensemble stage."""
+    import random
+    import torch
+    from masters_final_b200 import workloads as W
+    from masters_final_b200.utils.partition import generate_ensemble_labels
+    x = W.gaussian_mixture(500_000, 16, 50, seed=3, center_range=20.0, anisotropic=True)
+    X = torch.from_numpy(x).cuda()
+    np.random.seed(3)
+    random.seed(3)
+    for _ in range(2):
+        L, ks = generate_ensemble_labels(X, [350, 711], 20, 3, label_mode="bf16")
+    torch.cuda.synchronize()
+    return {"partitions": len(ks)}
+
+
 def case_mst_knn16_1M():
     """Three Boruvka MST calls on the 16-NN graph of 1,000,000 points."""
     import torch
@@ -886,7 +904,8 @@ def case_final_phase_synthetic():
     return {"entries": int(indptr[-1]), "n_fclusts": int(nc)}
 
 
-CASES = {"label_tc_100k": case_label_tc_100k, "mst_knn16_1M": case_mst_knn16_1M,
+CASES = {"label_tc_100k": case_label_tc_100k, "ensemble_500k_20p": case_ensemble_500k_20p,
+         "mst_knn16_1M": case_mst_knn16_1M,
          "coassoc300k": case_coassoc300k, "final_phase_synthetic": case_final_phase_synthetic}
 
 

@@ -404,6 +404,9 @@ static int launch_whist_u8(const uint8_t *w, int64_t n, unsigned long long *hist
 // slots with one atomicAdd, which keeps the shared cursor off the critical
 // path.  Edge order is not deterministic, results are: selection uses a
 // strict total order.
+// the final clustering merges its remaining weight phases once fewer than
+// one component per this many points is left
+constexpr int64_t kMergeBelow = 64;
 constexpr int kPhThreads = 256;
 constexpr int kPhWarps = kPhThreads / 32;
 
@@ -701,27 +704,45 @@ k_pick_giant(const int32_t *label, int64_t V0, int32_t *out)
 // Same for an upper-triangle CSR with uint8 weights: one word per kept entry,
 // offered to both ends.  Co-association rows are long (thousands of entries), so a
 // warp takes one row and walks it in 128-entry groups, each lane taking four
-// consecutive entries: their four weights (one word) are read first, and the
-// four column indices (16 bytes) only when one of the weights falls in the
-// phase's range, so a phase over a narrow range reads little more than the
-// weight array; only those entries gather the other end's label.  A first
-// walk (four groups in flight) counts the kept entries, the warp reserves
-// that many words with one atomic, and a second walk over the (now cached)
-// row writes them, runs of equal first end for the min-edge selection of
-// later rounds.  Each entry is checked (j > i, j < n) in the phase whose
-// range holds its weight.
-__global__ void __launch_bounds__(kPhThreads, 4)
+// consecutive entries: their four weights (one word) are read first and
+// tested against the phase's range four bytes at once, and the four column
+// indices (16 bytes) only when one of the weights falls in the range, so a
+// phase over a narrow range reads little more than the weight array; only
+// those entries gather the other end's label (none in the first phase, whose
+// labels are the identity).  Kept entries update the selection slots and the
+// per-weight counts as they are found and are staged in shared memory in walk
+// order; the warp then reserves the row's words with one atomic and copies
+// the staging out.  A row with more kept entries than the staging holds
+// walks again to write them.  Each entry is checked (j > i, j < n) in the
+// phase whose range holds its weight.
+constexpr int kUpStage = 128;      // staged edge words per warp
+
+// bit q: byte q of w lies in [L, H], with c1 = (0x8000 - L) and c2 = (0x7fff -
+// H) in both 16-bit halves: bytes 0, 2 and bytes 1, 3 are spread to 16-bit
+// lanes, where bit 15 of x + c1 is x >= L and bit 15 of x + c2 is x > H
+__device__ __forceinline__ unsigned bytes_in_range(uint32_t w, uint32_t c1, uint32_t c2)
+{
+    const uint32_t e = __byte_perm(w, 0u, 0x4240), o = __byte_perm(w, 0u, 0x4341);
+    const uint32_t me = (e + c1) & ~(e + c2), mo = (o + c1) & ~(o + c2);
+    return ((me >> 15) & 1u) | ((mo >> 14) & 2u) | ((me >> 29) & 4u) | ((mo >> 28) & 8u);
+}
+
+__global__ void __launch_bounds__(kPhThreads, 3)
 k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, int32_t n,
-              int64_t nnz, int lo, int hi, int dense, int64_t row0, int64_t row1,
+              int64_t nnz, int lo, int hi, int dense, int ident, int64_t row0, int64_t row1,
               const int32_t *label, Pack pk, uint64_t *eout, unsigned long long *cursor,
               unsigned long long cap, unsigned long long *best, unsigned long long *khist,
               int *err)
 {
     constexpr int G = 4;
     __shared__ unsigned s_kh[256];           // kept entries per weight, this block
+    __shared__ uint64_t stage_all[kPhWarps][kUpStage];
     for (int b = threadIdx.x; b < 256; b += blockDim.x) s_kh[b] = 0u;
     __syncthreads();
     const int lane = threadIdx.x & 31;
+    uint64_t *stage = stage_all[threadIdx.x >> 5];
+    const uint32_t c1 = 0x00010001u * (uint32_t)(0x8000 - (lo + 1));
+    const uint32_t c2 = 0x00010001u * (uint32_t)(0x7fff - hi);
     const int64_t nwarps = (int64_t)gridDim.x * kPhWarps;
     for (int64_t i = row0 + (int64_t)blockIdx.x * kPhWarps + (threadIdx.x >> 5); i < row1;
          i += nwarps) {
@@ -731,7 +752,7 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
             continue;
         }
         if (s == e_end) continue;
-        const int32_t li = label[i];
+        const int32_t li = ident ? (int32_t)i : label[i];
         const int64_t a0 = s & ~(int64_t)3;        // groups start on 16-byte index boundaries
         // weights of the lane's entries e .. e+3 (zero outside the arrays)
         auto wload = [&](int64_t e) -> uint32_t {
@@ -741,20 +762,16 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
             for (int q = 0; q < 4 && e + q < nnz; ++q) v |= (uint32_t)w[e + q] << (8 * q);
             return v;
         };
-        // bit q: entry e+q is in the row with its weight in (lo, hi]; four
-        // byte compares at once, the row's bounds only in its edge groups
-        const uint32_t lo4 = 0x01010101u * (uint32_t)(lo + 1), hi4 = 0x01010101u * (uint32_t)hi;
+        // bit q: entry e+q is in the row with its weight in (lo, hi]
         auto cmask = [&](int64_t e, uint32_t wv) -> unsigned {
-            uint32_t m = __vcmpgeu4(wv, lo4) & __vcmpleu4(wv, hi4);
+            unsigned m = bytes_in_range(wv, c1, c2);
             if (e < s || e + 4 > e_end) {
-                const int64_t a = s - e, b = e_end - e;     // valid bytes [a, b)
+                const int64_t a = s - e, b = e_end - e;     // valid entries [a, b)
                 const int qa = a < 0 ? 0 : (a > 4 ? 4 : (int)a);
                 const int qb = b < 0 ? 0 : (b > 4 ? 4 : (int)b);
-                const uint32_t va = qa >= 4 ? 0u : 0xffffffffu << (8 * qa);
-                const uint32_t vb = qb <= 0 ? 0u : 0xffffffffu >> (8 * (4 - qb));
-                m &= va & vb;
+                m &= (0xfu << qa) & (0xfu >> (4 - qb));
             }
-            return ((m >> 7) & 1u) | ((m >> 14) & 2u) | ((m >> 21) & 4u) | ((m >> 28) & 8u);
+            return m;
         };
         // the indices of the entries in cm (all four in a dense phase)
         auto jload = [&](int64_t e, unsigned cm) -> int4 {
@@ -770,22 +787,36 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
         // receives the candidates' other-end labels
         auto keep = [&](unsigned cm, const int4 &jv, int32_t (&lj)[4]) -> unsigned {
             const int32_t jj[4] = {jv.x, jv.y, jv.z, jv.w};
-            unsigned c2 = cm;
+            unsigned c2m = cm;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 if (((cm >> q) & 1u) && (jj[q] <= i || jj[q] >= n)) {
                     set_err(err, DEV_BAD_INPUT);
-                    c2 &= ~(1u << q);
+                    c2m &= ~(1u << q);
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) lj[q] = ((c2 >> q) & 1u) ? label[jj[q]] : li;
+            for (int q = 0; q < 4; ++q)
+                lj[q] = ((c2m >> q) & 1u) ? (ident ? jj[q] : label[jj[q]]) : li;
             unsigned km = 0u;
 #pragma unroll
             for (int q = 0; q < 4; ++q) km |= (lj[q] != li ? 1u : 0u) << q;
             return km;
         };
-        int cnt = 0;
+        // the row's kept words in walk order: warp prefix of the lanes' counts
+        auto place = [&](unsigned km, int c, int &tot) -> int {
+            int incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int o = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += o;
+            }
+            tot = __shfl_sync(0xffffffffu, incl, 31);
+            return incl - c;
+        };
+        int cnt = 0, staged = 0;
+        bool spill = false;
+        uint64_t m = kNone;
         for (int64_t g = a0; g < e_end; g += 128 * G) {
             uint32_t wv[G];
             unsigned cm[G];
@@ -812,57 +843,69 @@ k_phase_upper(const int64_t *indptr, const int32_t *indices, const uint8_t *w, i
 #pragma unroll
             for (int u = 0; u < G; ++u) {
                 int32_t lj[4];
-                const unsigned km = keep(cm[u], jv[u], lj);
-                cnt += __popc(km);
-                for (unsigned b = km; b; b &= b - 1u)
-                    atomicAdd(&s_kh[(wv[u] >> (8 * (__ffs(b) - 1))) & 255u], 1u);
+                const unsigned km = cm[u] ? keep(cm[u], jv[u], lj) : 0u;
+                if (!__any_sync(0xffffffffu, km != 0u)) continue;
+                const int c = __popc(km);
+                int tot;
+                int p = staged + place(km, c, tot);
+                if (staged + tot > kUpStage) spill = true;
+                const int32_t jj[4] = {jv[u].x, jv[u].y, jv[u].z, jv[u].w};
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (!((km >> q) & 1u)) continue;
+                    const uint32_t wq = (wv[u] >> (8 * q)) & 255u;
+                    const uint64_t k = pk.make(wq, (uint32_t)i, (uint32_t)jj[q]);
+                    atomicAdd(&s_kh[wq], 1u);
+                    m = (k >> 1) < m ? (k >> 1) : m;
+                    min_if_lower(&best[lj[q]], k >> 1);
+                    if (!spill) stage[p++] = k;
+                }
+                staged += tot;
+                cnt += c;
             }
         }
         cnt = __reduce_add_sync(0xffffffffu, cnt);
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
+            m = x < m ? x : m;
+        }
         if (cnt == 0) continue;
+        if (lane == 0 && m != kNone) min_if_lower(&best[li], m);
         unsigned long long at = 0;
         if (lane == 0) at = atomicAdd(cursor, (unsigned long long)cnt);
         at = __shfl_sync(0xffffffffu, at, 0);
         if (at + (unsigned long long)cnt > cap) {
             if (lane == 0) set_err(err, DEV_CAPACITY);
+            __syncwarp();
             continue;
         }
-        uint64_t m = kNone;
+        __syncwarp();
+        if (!spill) {
+            for (int t = lane; t < cnt; t += 32) eout[at + t] = stage[t];
+            __syncwarp();                  // the staging is reused by the next row
+            continue;
+        }
+        // more kept entries than the staging holds: walk again to write them
         for (int64_t g = a0; g < e_end; g += 128) {
             const int64_t e = g + 4 * lane;
             const uint32_t wv = wload(e);
             const unsigned cm = cmask(e, wv);
             const int4 jv = jload(e, cm);
             int32_t lj[4];
-            const unsigned km = keep(cm, jv, lj);
+            const unsigned km = cm ? keep(cm, jv, lj) : 0u;
+            if (!__any_sync(0xffffffffu, km != 0u)) continue;
             const int c = __popc(km);
-            int incl = c;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int o = __shfl_up_sync(0xffffffffu, incl, d);
-                if (lane >= d) incl += o;
-            }
-            const int tot = __shfl_sync(0xffffffffu, incl, 31);
-            if (tot == 0) continue;
-            unsigned long long p = at + (unsigned long long)(incl - c);
+            int tot;
+            unsigned long long p = at + (unsigned long long)place(km, c, tot);
             const int32_t jj[4] = {jv.x, jv.y, jv.z, jv.w};
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (!((km >> q) & 1u)) continue;
-                const uint64_t k = pk.make((wv >> (8 * q)) & 255u, (uint32_t)i, (uint32_t)jj[q]);
-                eout[p] = k;
-                m = (k >> 1) < m ? (k >> 1) : m;
-                min_if_lower(&best[lj[q]], k >> 1);
-                ++p;
-            }
+            for (int q = 0; q < 4; ++q)
+                if ((km >> q) & 1u)
+                    eout[p++] = pk.make((wv >> (8 * q)) & 255u, (uint32_t)i, (uint32_t)jj[q]);
             at += (unsigned long long)tot;
         }
-#pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) {
-            const uint64_t x = __shfl_xor_sync(0xffffffffu, m, o);
-            m = x < m ? x : m;
-        }
-        if (lane == 0 && m != kNone) min_if_lower(&best[li], m);
+        __syncwarp();
     }
     __syncthreads();
     for (int b = threadIdx.x; b < 256; b += blockDim.x)
@@ -875,6 +918,7 @@ struct Phase {
     int lo, hi;
     int64_t r0, r1;
     int slot;
+    int ident;            // the labels are still the identity (no merges yet)
 };
 
 // Phase ranges (lo, hi] of weight buckets: cut the bucket histogram at the
@@ -1789,7 +1833,9 @@ struct Engine {
         for (size_t q = 0; q < plan.size(); ++q) {
             EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V0, st));
             EACB_CUDA(cudaMemsetAsync(&cnt[C_CURSOR], 0, sizeof(int64_t), st));
-            int s = build(plan[q]);
+            Phase ph = plan[q];
+            ph.ident = q == 0;                 // no round has merged anything yet
+            int s = build(ph);
             if (s) return s;
             k_phase_begin<<<1, 32, 0, st>>>(cnt, V0, q == 0 ? 1 : 0);
             EACB_CHECK_LAUNCH();
@@ -1813,8 +1859,10 @@ struct Engine {
     {
         int64_t V = V0, n_mst = 0;
         size_t q = 0;
+        bool merged = false;
         while (q < plan.size()) {
-            const Phase ph = plan[q];
+            Phase ph = plan[q];
+            ph.ident = !merged;                // no round has merged anything yet
             EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V, st));
             EACB_CUDA(cudaMemsetAsync(&cnt[C_CURSOR], 0, sizeof(int64_t), st));
             EACB_CUDA(cudaMemsetAsync(hist, 0, 256 * sizeof(unsigned long long), st));
@@ -1844,9 +1892,25 @@ struct Engine {
             if (prof().enabled) prof().bytes[PROF_PHASE] += 8.0 * (double)Ep;   // words written
             int64_t nc = 0;
             if ((s = run<SEL_MST>(pk, Ep, V, st, &n_mst, &nc))) return s;
+            merged = merged || nc < V;
             V = nc;
             ++q;
             if (V <= 1) break;
+            // Few components left: the rest of the weights in one phase.
+            // Each phase walks the whole matrix, and once the components are
+            // few most entries join a component to itself, so the remaining
+            // phases would keep few words each; a merged phase that does
+            // overflow the edge array is redone in pieces like any other.
+            if (q + 1 < plan.size() && V * kMergeBelow <= V0) {
+                bool full = true;
+                for (size_t r = q; r < plan.size(); ++r)
+                    full = full && plan[r].r0 == 0 && plan[r].r1 == V0;
+                if (full) {
+                    const Phase rest{plan[q].lo, plan.back().hi, 0, V0, -1, 0};
+                    plan.resize(q);
+                    plan.push_back(rest);
+                }
+            }
         }
         *n_mst_out = n_mst;
         *n_comp_out = V;
@@ -2339,7 +2403,8 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
         if (nnz == 0) return EACB_OK;
         ProfScope ps(PROF_PHASE, st);
         k_phase_upper<<<grid_for((ph.r1 - ph.r0) * 32, kPhThreads), kPhThreads, 0, st>>>(
-            indptr, indices, diassoc, n, nnz, ph.lo, ph.hi, dense(ph), ph.r0, ph.r1, g.label, pk, g.ea,
+            indptr, indices, diassoc, n, nnz, ph.lo, ph.hi, dense(ph), ph.ident, ph.r0, ph.r1,
+            g.label, pk, g.ea,
             (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best, g.hist,
             g.err);
         EACB_CHECK_LAUNCH();
