@@ -358,14 +358,16 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
                 ncv[4 * q + 2] = f.z;
                 ncv[4 * q + 3] = f.w;
             }
+            // the screened distance less the row's |x|^2 (the same for every
+            // column, so the order and the gaps are those of the distance):
+            // one rounding, where adding |x|^2 first would take two
+            const int cb = t * kTN + c0;
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
-                const int c = c0 + j;
-                const float s = fmaf(-2.f, v[j], xn + ncv[j]);   // ncp[c] = +inf past K
-                const bool lt = s < b1;
-                b2 = lt ? b1 : fminf(b2, s);
-                i1 = lt ? t * kTN + c : i1;
-                b1 = lt ? s : b1;
+                const float s = fmaf(-2.f, v[j], ncv[j]);        // ncp[c] = +inf past K
+                i1 = s < b1 ? cb + j : i1;
+                b2 = fminf(b2, fmaxf(b1, s));
+                b1 = fminf(b1, s);
             }
         }
         tc_fence_before();
@@ -448,35 +450,115 @@ __global__ void k_exact_all(const float *__restrict__ X, int32_t n, int32_t D,
         if (active[o / n]) exact_label_point(X, n, D, C, kk, kmax, o, labels, dists);
 }
 
-__global__ void k_label_exact_tc(const float *__restrict__ X, int32_t n, int32_t D,
-                                 const float *__restrict__ C, const int32_t *__restrict__ kk,
-                                 int32_t kmax, int32_t P, const int32_t *__restrict__ amb,
-                                 const int *__restrict__ namb, const int *__restrict__ err,
-                                 int32_t *labels, float *dists)
+// The reference's distance sum_d (double) fl(fl(x_d - c_d)^2) and the FP32
+// sum of the same squares by fused multiply-adds differ by at most (D + 2)
+// 2^-24 of either (the squares round once, the chain once per term; the
+// double sum adds < D 2^-53), plus subnormal rounding far below 1e-38.  So
+// every centroid that can hold the reference's minimum -- and every one tied
+// with it -- has an FP32 sum within (1 + 4 (D + 2) 2^-24) of the smallest
+// FP32 sum, with a factor 2 to spare.
+// a centroid row into registers: four floats at a time when D is a
+// multiple of four (rows then start on 16-byte boundaries)
+template <int DM, bool VEC>
+__device__ __forceinline__ void load_row(const float *c, int D, float (&v)[DM])
 {
+    if (VEC) {
+#pragma unroll
+        for (int d = 0; d < DM; d += 4) {
+            const float4 f = __ldg(reinterpret_cast<const float4 *>(c + d));
+            v[d] = f.x;
+            v[d + 1] = f.y;
+            v[d + 2] = f.z;
+            v[d + 3] = f.w;
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < DM; ++d) v[d] = d < D ? __ldg(c + d) : 0.f;
+    }
+}
+
+template <int DM>
+__device__ __forceinline__ float screen_dist(const float (&x)[DM], const float (&c)[DM], int D)
+{
+    float acc = 0.f;
+#pragma unroll
+    for (int d = 0; d < DM; ++d)
+        if (d < D) {
+            const float diff = __fsub_rn(x[d], c[d]);
+            acc = __fmaf_rn(diff, diff, acc);
+        }
+    return acc;
+}
+
+template <int DM>
+__device__ __forceinline__ double exact_dist_reg(const float (&x)[DM], const float (&c)[DM], int D)
+{
+    double dist = 0.0;
+#pragma unroll
+    for (int d = 0; d < DM; ++d)
+        if (d < D) {
+            const float diff = __fsub_rn(x[d], c[d]);
+            dist = __dadd_rn(dist, (double)__fmul_rn(diff, diff));
+        }
+    return dist;
+}
+
+constexpr int kExactThreads = 256;
+constexpr int kExactCacheK = 2048;     // FP32 sums kept in shared memory up to this k
+
+// One warp per ambiguous point, lane l over centroids l, l + 32, ...: an FP32
+// pass finds the smallest sum (keeping each sum in shared memory when k is at
+// most kExactCacheK), a second pass evaluates the reference's arithmetic only
+// for the centroids within the bound above, and the warp keeps the smallest
+// distance, the smallest index among equal ones (the reference loop's first
+// minimum).
+template <int DM, bool VEC>
+__global__ void __launch_bounds__(kExactThreads)
+k_label_exact_tc(const float *__restrict__ X, int32_t n, int32_t D, const float *__restrict__ C,
+                 const int32_t *__restrict__ kk, int32_t kmax, int32_t P,
+                 const int32_t *__restrict__ amb, const int *__restrict__ namb,
+                 const int *__restrict__ err, int32_t *labels, float *dists)
+{
+    extern __shared__ float s_sum[];
     if (*err != 0) return;                      // k_exact_all did every point
     const int64_t cap = (int64_t)P * n;
     const int m = (int)min((int64_t)*namb, cap);
-    // one warp per point: lane l evaluates centroids l, l + 32, ... with the
-    // reference's arithmetic, and the warp keeps the smallest distance, the
-    // smallest index among equal ones (the reference loop's first minimum)
+    const float grow = 1.f + 4.f * (float)(D + 2) * 5.9604645e-8f;     // 2^-24
+    const bool cached = kmax <= kExactCacheK;
+    float *mine = s_sum + (threadIdx.x >> 5) * (cached ? kmax : 0);
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < m; t += nw) {
         const int64_t o = amb[t];
         const int64_t p = o / n, i = o - p * n;
         const int K = kk[p];
-        const float *x = X + i * D;
+        float xv[DM], cv[DM];
+        load_row<DM, VEC>(X + i * D, D, xv);
         const float *Cp = C + p * kmax * D;
+        float mn = __int_as_float(0x7f800000);
+        for (int k = lane; k < K; k += 32) {
+            load_row<DM, VEC>(Cp + (int64_t)k * D, D, cv);
+            const float d32 = screen_dist<DM>(xv, cv, D);
+            if (cached) mine[k] = d32;
+            mn = fminf(mn, d32);
+        }
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, off));
+        const float thr = __fadd_ru(__fmul_ru(mn, grow), 1e-38f);
         double best = 0.0;
         int bl = 0x7fffffff;
         for (int k = lane; k < K; k += 32) {
-            double dist = 0.0;
-            for (int d = 0; d < D; ++d) {
-                const float diff = __fsub_rn(x[d], Cp[(int64_t)k * D + d]);
-                dist = __dadd_rn(dist, (double)__fmul_rn(diff, diff));
+            float d32;
+            if (cached) {
+                d32 = mine[k];
+            } else {
+                load_row<DM, VEC>(Cp + (int64_t)k * D, D, cv);
+                d32 = screen_dist<DM>(xv, cv, D);
             }
-            if (k == lane || dist < best) {
+            if (d32 > thr) continue;
+            load_row<DM, VEC>(Cp + (int64_t)k * D, D, cv);
+            const double dist = exact_dist_reg<DM>(xv, cv, D);
+            if (bl == 0x7fffffff || dist < best) {
                 best = dist;
                 bl = k;
             }
@@ -494,6 +576,7 @@ __global__ void k_label_exact_tc(const float *__restrict__ X, int32_t n, int32_t
             labels[o] = bl;
             dists[o] = (float)best;
         }
+        __syncwarp();                           // the sums are rewritten by the next point
     }
 }
 
@@ -573,8 +656,28 @@ int label_pass_tc(const float *X, int32_t n, int32_t D, int32_t P, const float *
     ps.done(0.0);
     k_exact_all<<<296, 256, 0, st>>>(X, n, D, C, kk, kmax, P, active, s.err, labels, dists);
     EACB_CHECK_LAUNCH();
-    k_label_exact_tc<<<148 * 8, 256, 0, st>>>(X, n, D, C, kk, kmax, P, amb, namb, s.err, labels,
-                                              dists);
+    const size_t esmem = kmax <= kExactCacheK
+                             ? (size_t)(kExactThreads / 32) * kmax * sizeof(float) : 0;
+    int es = EACB_OK;
+    auto exact = [&](auto kern) {
+        if (esmem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)esmem) != cudaSuccess)
+            es = EACB_ERR_CUDA;
+        else
+            kern<<<148 * 8, kExactThreads, esmem, st>>>(X, n, D, C, kk, kmax, P, amb, namb, s.err,
+                                                        labels, dists);
+    };
+    // 16-byte row loads when every row is exactly DM floats on a 16-byte boundary
+    const bool al = ((uintptr_t)X % 16 == 0) && ((uintptr_t)C % 16 == 0);
+    if (D == 4 && al) exact(k_label_exact_tc<4, true>);
+    else if (D <= 4) exact(k_label_exact_tc<4, false>);
+    else if (D == 8 && al) exact(k_label_exact_tc<8, true>);
+    else if (D <= 8) exact(k_label_exact_tc<8, false>);
+    else if (D == 16 && al) exact(k_label_exact_tc<16, true>);
+    else if (D <= 16) exact(k_label_exact_tc<16, false>);
+    else if (D == 32 && al) exact(k_label_exact_tc<32, true>);
+    else exact(k_label_exact_tc<32, false>);
+    if (es) return es;
     EACB_CHECK_LAUNCH();
     return EACB_OK;
 }
