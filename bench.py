@@ -605,6 +605,21 @@ def eac_measurements(args):
                         "ms_ensemble": tot[0] / steps, "ms_coassoc": tot[1] / steps,
                         "ms_mst_cut": tot[2] / steps}
             parts[key] = labels
+        if not small:
+            # the same BF16 run with the built-in launch shapes instead of the
+            # autotuner's table
+            from masters_final_b200 import _lib
+            _lib.clear_tuning()
+            try:
+                e = L = None
+                flush.fill_(1)
+                ms_u, _, e, L = eac_run_once(X, cfg, "bf16", torch)
+            finally:
+                _lib.apply_tuning()
+            res["bf16_tc_untuned"] = {"points_per_s": cfg["n"] / (sum(ms_u) / 1000.0),
+                                      "ms": sum(ms_u), "ms_ensemble": ms_u[0],
+                                      "ms_coassoc": ms_u[1], "ms_mst_cut": ms_u[2],
+                                      "tuning": "built-in defaults (table cleared)"}
         res["identical_partitions"] = bool(np.array_equal(parts["bf16_tc"], parts["fp32"]))
         res["nnz"] = int(e.coassoc.nnz)
         res["nnz_discarded"] = int(e.coassoc.nnz_discarded)
@@ -765,14 +780,27 @@ def eac_batched_measurement(torch, args):
     xs = W.batched_instances(cfg["instances"], seed=cfg["seed"])
     ps = [draw_instance_params(x.shape[0], k_range_rule1(x.shape[0]), cfg["P"], i)
           for i, x in enumerate(xs)]
+    from masters_final_b200 import _lib
     Xd = [torch.from_numpy(x).cuda() for x in xs]
     N = int(sum(x.shape[0] for x in xs))
-    eac_batch(Xd, params=ps, n_workers=cfg["workers"], return_device=True)
+    workers = int(_lib.tuned("batched_workers", cfg["workers"]))
+    eac_batch(Xd, params=ps, n_workers=workers, return_device=True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    r = eac_batch(Xd, params=ps, n_workers=cfg["workers"], return_device=True)
+    r = eac_batch(Xd, params=ps, n_workers=workers, return_device=True)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
+    # untuned: the built-in launch shapes and the default worker count
+    _lib.clear_tuning()
+    try:
+        eac_batch(Xd, params=ps, return_device=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eac_batch(Xd, params=ps, return_device=True)
+        torch.cuda.synchronize()
+        du = time.perf_counter() - t0
+    finally:
+        _lib.apply_tuning()
     st = np.array([a.ms_stages for a in r])
     out = {"points_per_s": N / dt, "s": dt, "sum_n": N, "instances": len(xs),
            "nnz_total": int(sum(a.nnz for a in r)),
@@ -780,8 +808,11 @@ def eac_batched_measurement(torch, args):
            "failed": int(sum(a.status != 0 for a in r)),
            "worker_ms_sums": {"ensemble": float(st[:, 0].sum()), "coassoc": float(st[:, 1].sum()),
                               "final": float(st[:, 2].sum())},
-           "config": {**cfg, "n_range": [1000, 50000], "d": [2, 4, 8, 16, 32],
-                      "gaussians": [3, 30], "sigma": [0.5, 2.0], "label_mode": "bf16"}}
+           "untuned": {"points_per_s": N / du, "s": du,
+                       "tuning": "built-in defaults (table cleared, default worker count)"},
+           "config": {**cfg, "workers": workers, "n_range": [1000, 50000],
+                      "d": [2, 4, 8, 16, 32], "gaussians": [3, 30], "sigma": [0.5, 2.0],
+                      "label_mode": "bf16"}}
     # the plain single-instance pipeline: FP32 labeler, one dataset at a time
     def single(i):
         np.random.seed(i)

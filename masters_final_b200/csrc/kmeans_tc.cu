@@ -4,8 +4,8 @@
 // products run as ONE BF16 GEMM with FP32 accumulation in tensor memory:
 // each float32 operand is split into three BF16 parts (h + m + l, ~24
 // significant bits) and the K dimension holds the six products that matter
-// (see put_row), the large h*h group last.  The epilogue (8 warps, one point
-// row per thread, half the columns per warp pair) reads the accumulator tile
+// (see put_row), the large h*h group last.  The epilogue (16 warps, one point
+// row per thread, a quarter of the columns per warp) reads the accumulator tile
 // from TMEM with tcgen05.ld, forms the screened distance and keeps the best
 // two per point.  A point whose runner-up lies within the proven error bound
 // E (|x|^2 + max|c|^2) of its winner (E from the split, the accumulation
@@ -31,7 +31,9 @@ namespace eacb {
 
 constexpr int kTM = 128;           // points per CTA tile
 constexpr int kTN = 256;           // centroids per MMA tile
-constexpr int kTThreads = 256;     // 8 warps
+constexpr int kTThreads = 512;     // 16 warps: 4 TMEM lane quarters x 4 column quarters
+constexpr int kTColGroups = kTThreads / kTM;
+constexpr int kTColsPer = kTN / kTColGroups;
 constexpr int kTmemCols = 256;
 constexpr int kWaitLimit = 1 << 26;
 
@@ -133,6 +135,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
+
+__host__ __device__ __forceinline__ uint32_t sbo_b(int Kp) { return 128u * (uint32_t)(Kp >> 3); }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -245,7 +249,7 @@ __global__ void k_prep_centroids(const float *C, const int32_t *kk, int32_t kmax
 // ---------------------------------------------------------------- labels --
 __global__ void __launch_bounds__(kTThreads, 2)
 k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const float *__restrict__ C,
-           const int32_t *__restrict__ kk, int32_t kmax, int32_t kt_max,
+           const int32_t *__restrict__ kk, int32_t kmax, int32_t kt_max, int32_t P, int32_t ppc,
            const int32_t *__restrict__ active, const uint8_t *__restrict__ A,
            const float *__restrict__ nx, const uint8_t *__restrict__ B,
            const float *__restrict__ nc, const float *__restrict__ cmax2, float E, int nbuf,
@@ -254,23 +258,34 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t bar_a, bar_b[2], bar_mma;
     __shared__ uint32_t tmem_slot;
-    __shared__ float s_b1[kTM], s_b2[kTM];
-    __shared__ int s_i1[kTM];
+    __shared__ float s_b1[kTColGroups - 1][kTM], s_b2[kTColGroups - 1][kTM];
+    __shared__ int s_i1[kTColGroups - 1][kTM];
     __shared__ int s_fail;
-    const int p = blockIdx.y;
-    if (!active[p]) return;
-    const int K = kk[p];
-    const int tiles = (K + kTN - 1) / kTN;
     const uint32_t a_bytes = (uint32_t)kTM * Kp * 2, b_bytes = (uint32_t)kTN * Kp * 2;
     uint8_t *sA = smem;
     // two centroid-tile buffers when they fit (prefetch overlaps the MMA),
     // else one (prefetch overlaps the epilogue)
     uint8_t *sB[2] = {smem + a_bytes, nbuf == 2 ? smem + a_bytes + b_bytes : smem + a_bytes};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // the MMA issuer: a thread of the last warp, which has no per-partition
+    // tail, so the next MMA starts while the first warps finish a partition
+    const bool issuer = threadIdx.x == kTThreads - 32;
     const int64_t tile0 = blockIdx.x;
     const uint8_t *Ap = A + tile0 * a_bytes;
-    const uint8_t *Bp = B + (int64_t)p * kt_max * b_bytes;
+    // the tiles in order: every centroid tile of every active partition of
+    // this CTA's share [pb, pe) of the partitions
+    const int pb = blockIdx.y * ppc, pe = min(P, pb + ppc);
+    auto ntiles = [&](int q) -> int { return active[q] ? (kk[q] + kTN - 1) / kTN : 0; };
+    auto first_from = [&](int q) -> int {
+        while (q < pe && ntiles(q) == 0) ++q;
+        return q < pe ? q : P;
+    };
+    auto btile = [&](int q, int t) -> const uint8_t * {
+        return B + ((int64_t)q * kt_max + t) * b_bytes;
+    };
 
+    int p = first_from(pb);
+    if (p >= P) return;                          // uniform: nothing to label
     if (threadIdx.x == 0) {
         s_fail = 0;
         mbar_init(&bar_a, 1);
@@ -290,44 +305,57 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
 
-    if (threadIdx.x == 0) {
+    if (issuer) {
         mbar_expect_tx(&bar_a, a_bytes);
         bulk_g2s(sA, Ap, a_bytes, &bar_a);
         mbar_expect_tx(&bar_b[0], b_bytes);
-        bulk_g2s(sB[0], Bp, b_bytes, &bar_b[0]);
+        bulk_g2s(sB[0], btile(p, 0), b_bytes, &bar_b[0]);
     }
-    // epilogue ownership: row = 32*(warp%4) + lane, columns [128*(warp/4), +128)
+    // epilogue ownership: row = 32*(warp%4) + lane (the TMEM lanes warp w may
+    // read), columns [64*(warp/4), +64)
     const int row = 32 * (warp & 3) + lane;
-    const int colh = 128 * (warp >> 2);
+    const int cgrp = warp >> 2, colh = kTColsPer * cgrp;
     const int64_t i = tile0 * kTM + row;
     const float xn = (i < n) ? nx[i] : 0.f;
     float b1 = __int_as_float(0x7f800000), b2 = b1;
     int i1 = 0;
     const uint32_t lbo = 128, sbo = 128u * (uint32_t)(Kp >> 3);
     uint32_t ph_b[2] = {0, 0}, ph_mma = 0;
+    int pend = -1;                               // buffer with a copy in flight (issuer)
+    int mma_ph = -1;                             // phase of an MMA not yet seen complete
     bool ok = true;
-    for (int t = 0; t < tiles && ok; ++t) {
-        const int buf = nbuf == 2 ? (t & 1) : 0;
-        const int nvalid = min(kTN, K - t * kTN);
+    int t = 0, tiles = ntiles(p);
+    for (int64_t j = 0; p < P; ++j) {
+        // the tile after (p, t): its copy is issued while this one is used
+        int pn = p, tn = t + 1;
+        if (tn == tiles) {
+            pn = first_from(p + 1);
+            tn = 0;
+        }
+        const int buf = nbuf == 2 ? (int)(j & 1) : 0;
+        const int nvalid = min(kTN, kk[p] - t * kTN);
         const int N = (nvalid + 15) & ~15;
-        if (threadIdx.x == 0) {
-            bool got = (t == 0 ? mbar_wait(&bar_a, 0) : true) && mbar_wait(&bar_b[buf], ph_b[buf]);
+        if (issuer) {
+            bool got = (j == 0 ? mbar_wait(&bar_a, 0) : true) && mbar_wait(&bar_b[buf], ph_b[buf]);
             if (!got) {
                 set_err(err, DEV_SPIN_LIMIT);
                 s_fail = 1;
             } else {
+                pend = -1;
                 tc_fence_after();
                 const uint32_t idesc = umma_idesc(kTM, N);
                 for (int s = 0; s < (Kp >> 4); ++s) {
                     const uint64_t ad = umma_desc(sA + s * 256, lbo, sbo);
-                    const uint64_t bd = umma_desc(sB[buf] + s * 256, lbo, 128u * (uint32_t)(Kp >> 3));
+                    const uint64_t bd = umma_desc(sB[buf] + s * 256, lbo, sbo_b(Kp));
                     mma_bf16(tmem, ad, bd, idesc, s > 0 ? 1u : 0u);
                 }
                 mma_commit(&bar_mma);
-                if (nbuf == 2 && t + 1 < tiles) {
-                    // the other buffer's last reader (MMA of tile t-1) completed
+                mma_ph = (int)ph_mma;
+                if (nbuf == 2 && pn < P) {
+                    // the other buffer's last reader (the previous MMA) completed
                     mbar_expect_tx(&bar_b[buf ^ 1], b_bytes);
-                    bulk_g2s(sB[buf ^ 1], Bp + (int64_t)(t + 1) * b_bytes, b_bytes, &bar_b[buf ^ 1]);
+                    bulk_g2s(sB[buf ^ 1], btile(pn, tn), b_bytes, &bar_b[buf ^ 1]);
+                    pend = buf ^ 1;
                 }
             }
         }
@@ -337,15 +365,19 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
         if (!mbar_wait(&bar_mma, ph_mma)) {
             set_err(err, DEV_SPIN_LIMIT);
             s_fail = 1;
-        } else if (nbuf == 1 && threadIdx.x == 0 && t + 1 < tiles) {
-            // single buffer: this tile's MMA has finished reading it
-            mbar_expect_tx(&bar_b[0], b_bytes);
-            bulk_g2s(sB[0], Bp + (int64_t)(t + 1) * b_bytes, b_bytes, &bar_b[0]);
+        } else if (issuer) {
+            mma_ph = -1;
+            if (nbuf == 1 && pn < P) {
+                // single buffer: this tile's MMA has finished reading it
+                mbar_expect_tx(&bar_b[0], b_bytes);
+                bulk_g2s(sB[0], btile(pn, tn), b_bytes, &bar_b[0]);
+                pend = 0;
+            }
         }
         ph_mma ^= 1;
         tc_fence_after();
         const float *ncp = nc + ((int64_t)p * kt_max + t) * kTN;
-        const int c_lo = colh, c_hi = min(colh + 128, nvalid);
+        const int c_lo = colh, c_hi = min(colh + kTColsPer, nvalid);
         for (int c0 = c_lo; c0 < c_hi; c0 += 16) {
             float v[16], ncv[16];
             tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c0, v);
@@ -363,46 +395,66 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
             // one rounding, where adding |x|^2 first would take two
             const int cb = t * kTN + c0;
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const float s = fmaf(-2.f, v[j], ncv[j]);        // ncp[c] = +inf past K
-                i1 = s < b1 ? cb + j : i1;
-                b2 = fminf(b2, fmaxf(b1, s));
-                b1 = fminf(b1, s);
+            for (int jj = 0; jj < 16; ++jj) {
+                const float sv = fmaf(-2.f, v[jj], ncv[jj]);      // ncp[c] = +inf past K
+                i1 = sv < b1 ? cb + jj : i1;
+                b2 = fminf(b2, fmaxf(b1, sv));
+                b1 = fminf(b1, sv);
             }
         }
         tc_fence_before();
-        __syncthreads();
-        if (s_fail) ok = false;
-    }
-    // merge the two column halves of each row
-    if (warp >= 4) {
-        s_b1[row] = b1;
-        s_b2[row] = b2;
-        s_i1[row] = i1;
-    }
-    __syncthreads();
-    if (warp < 4 && ok && i < n) {
-        const float o1 = s_b1[row], o2 = s_b2[row];
-        const int oi = s_i1[row];
-        // the lower index wins equal screened values; equal values are a
-        // near tie anyway and go to the exact re-check below
-        float w1, w2;
-        int wi;
-        if (o1 < b1) { w1 = o1; wi = oi; w2 = fminf(b1, o2); }
-        else { w1 = b1; wi = i1; w2 = fminf(o1, b2); }
-        // each screened distance is within E/2 (|x|^2 + max|c|^2) of the
-        // exact one (E carries a factor 2 of margin): the winner is certain
-        // when the runner-up is more than twice that above it
-        const float bound = E * (xn + cmax2[p]);
-        const int64_t o = (int64_t)p * n + i;
-        if (w2 - w1 > bound) {
-            float xv[32];
-            for (int d = 0; d < D; ++d) xv[d] = X[i * D + d];
-            labels[o] = wi;
-            dists[o] = (float)exact_dist<32>(xv, C + ((int64_t)p * kmax + wi) * D, D);
-        } else {
-            amb[atomicAdd(namb, 1)] = (int32_t)o;
+        __syncthreads();                         // the accumulator is free again
+        if (s_fail) { ok = false; break; }
+        if (t + 1 == tiles) {
+            // the partition is done: merge the column quarters of each row, in
+            // column order
+            if (cgrp > 0) {
+                s_b1[cgrp - 1][row] = b1;
+                s_b2[cgrp - 1][row] = b2;
+                s_i1[cgrp - 1][row] = i1;
+            }
+            __syncthreads();
+            if (cgrp == 0 && i < n) {
+                // the lower index wins equal screened values; equal values are
+                // a near tie anyway and go to the exact re-check
+                float w1 = b1, w2 = b2;
+                int wi = i1;
+#pragma unroll
+                for (int q = 0; q < kTColGroups - 1; ++q) {
+                    const float o1 = s_b1[q][row], o2 = s_b2[q][row];
+                    if (o1 < w1) {
+                        w2 = fminf(w1, o2);
+                        w1 = o1;
+                        wi = s_i1[q][row];
+                    } else {
+                        w2 = fminf(w2, o1);
+                    }
+                }
+                // each screened distance is within E/2 (|x|^2 + max|c|^2) of
+                // the exact one (E carries a factor 2 of margin): the winner is
+                // certain when the runner-up is more than twice that above it
+                const float bound = E * (xn + cmax2[p]);
+                const int64_t o = (int64_t)p * n + i;
+                if (w2 - w1 > bound) {
+                    float xv[32];
+                    for (int d = 0; d < D; ++d) xv[d] = X[i * D + d];
+                    labels[o] = wi;
+                    dists[o] = (float)exact_dist<32>(xv, C + ((int64_t)p * kmax + wi) * D, D);
+                } else {
+                    amb[atomicAdd(namb, 1)] = (int32_t)o;
+                }
+            }
+            b1 = b2 = __int_as_float(0x7f800000);
+            i1 = 0;
         }
+        p = pn;
+        t = tn;
+        if (tn == 0 && pn < P) tiles = ntiles(pn);
+    }
+    if (!ok && issuer) {
+        // leave no copy or MMA writing into this CTA's memory (bounded waits)
+        if (pend >= 0) mbar_wait(&bar_b[pend], ph_b[pend]);
+        if (mma_ph >= 0) mbar_wait(&bar_mma, (uint32_t)mma_ph);
     }
     tc_fence_before();
     __syncthreads();
@@ -647,9 +699,16 @@ int label_pass_tc(const float *X, int32_t n, int32_t D, int32_t P, const float *
     const size_t floor_bytes = ctas == 2 ? 100 * 1024 : 120 * 1024;
     const size_t smem_req = smem < floor_bytes ? floor_bytes : smem;
     EACB_CUDA(allow_max_dyn_smem(k_label_tc));
-    dim3 grid((unsigned)(s.n_pad / kTM), (unsigned)P);
+    // one CTA per 128-point tile and share of the partitions: all partitions
+    // (the tile's operands load once) unless that leaves fewer than two
+    // CTAs per SM slot in flight
+    const int64_t ptiles = s.n_pad / kTM;
+    const int64_t want = 2 * 148 * ctas;
+    const int groups = (int)std::min<int64_t>(P, std::max<int64_t>(1, (want + ptiles - 1) / ptiles));
+    const int ppc = (P + groups - 1) / groups;
+    dim3 grid((unsigned)ptiles, (unsigned)((P + ppc - 1) / ppc));
     ProfScope ps(PROF_KMEANS, st);
-    k_label_tc<<<grid, kTThreads, smem_req, st>>>(X, n, D, s.Kp, C, kk, kmax, s.kt_max, active,
+    k_label_tc<<<grid, kTThreads, smem_req, st>>>(X, n, D, s.Kp, C, kk, kmax, s.kt_max, P, ppc, active,
                                                   s.A, s.nx, s.B, s.nc, s.cmax2, E, nbuf, labels, dists,
                                                   amb, namb, s.err);
     EACB_CHECK_LAUNCH();
