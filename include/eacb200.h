@@ -86,7 +86,9 @@ void eacb_profile_read(int64_t *launches, double *ms, double *bytes, int64_t *co
  * per SM, 4 the graph MST's first weight phase as a share of the entries
  * in per mille (a = 0, b = vertices), 5 the Boruvka round kernel's
  * participants at most (a = 0 graph MST/CC, 1 EAC final clustering;
- * b = vertices).  eacb_tune_set adds an entry for a <= .. <= a_hi and
+ * b = vertices), 6 the co-association pair tiles: the compare work a group
+ * may take per member visit of the streaming kernels (0: streaming only;
+ * a = P, b = n).  eacb_tune_set adds an entry for a <= .. <= a_hi and
  * b_lo <= .. <= b_hi (the first matching entry wins); eacb_tune_clear
  * removes all; eacb_tune_get returns the value a launch of shape (a, b)
  * would use (dflt when no entry matches).  Process-wide; set it between
