@@ -877,6 +877,23 @@ def case_ensemble_500k_20p():
     return {"partitions": len(ks)}
 
 
+def case_batched_64():
+    """Batched EAC of every eighth of the 512 datasets (64 instances, n
+    from 1,000 to 50,000, 50 partitions, BF16 labels), two calls."""
+    import torch
+    from masters_final_b200 import workloads as W
+    from masters_final_b200.EAC.batched import draw_instance_params, eac_batch, k_range_rule1
+    xs = W.batched_instances(EAC_BATCHED["instances"], seed=EAC_BATCHED["seed"])
+    ps = [draw_instance_params(x.shape[0], k_range_rule1(x.shape[0]), EAC_BATCHED["P"], i)
+          for i, x in enumerate(xs)][::8]
+    Xd = [torch.from_numpy(x).cuda() for x in xs[::8]]
+    for _ in range(2):
+        r = eac_batch(Xd, params=ps, return_device=True)
+    torch.cuda.synchronize()
+    return {"instances": len(Xd), "sum_n": int(sum(x.shape[0] for x in Xd)),
+            "failed": int(sum(a.status != 0 for a in r))}
+
+
 def case_mst_knn16_1M():
     """Three Boruvka MST calls on the 16-NN graph of 1,000,000 points."""
     import torch
@@ -936,7 +953,7 @@ def case_final_phase_synthetic():
 
 
 CASES = {"label_tc_100k": case_label_tc_100k, "ensemble_500k_20p": case_ensemble_500k_20p,
-         "mst_knn16_1M": case_mst_knn16_1M,
+         "batched_64": case_batched_64, "mst_knn16_1M": case_mst_knn16_1M,
          "coassoc300k": case_coassoc300k, "final_phase_synthetic": case_final_phase_synthetic}
 
 

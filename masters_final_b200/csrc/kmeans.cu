@@ -316,10 +316,12 @@ __global__ void k_centroids(const float *__restrict__ X, int32_t n, int32_t D,
 //   the m-th back small      -> position of F[a_m],
 //   a back big B[u]          -> position of B[u + 1],
 // and r = lo + (number of smalls that landed).  Ranges up to kFillSeqMax
-// elements finish with the reference's loop on one thread.
+// elements finish with the reference's loop on one thread: its dependent
+// loads cost about as much per element as a parallel step costs per range,
+// so the handover is at a few hundred elements.
 constexpr int kFillThreads = 1024;
 constexpr int kFillItems = 8;
-constexpr int64_t kFillSeqMax = 16384;
+constexpr int64_t kFillSeqMax = 256;
 constexpr int64_t kFillInf = (int64_t)1 << 62;
 
 // Walks [lo, hi] in ascending order, calling f(p, big, bigs_before) for every

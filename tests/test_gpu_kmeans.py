@@ -78,6 +78,29 @@ def test_fit_f64_centroids_and_empty_clusters(T):
             assert int(it[p].item()) == ri
 
 
+@pytest.mark.parametrize("n", [300, 1000, 2500])
+def test_fit_empty_clusters_small_n(T, n):
+    """Empty clusters at the batched workload's instance sizes: the range
+    above the one-thread limit runs the block-parallel partition steps, which
+    must reproduce the reference's selection order (three duplicated initial
+    points, so three clusters empty out in the first pass)."""
+    from masters_final_b200.cluster.KMeans import kmeans_ensemble
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal((n, 3)).astype(np.float32)
+    x[1], x[3], x[5] = x[0], x[2], x[4]
+    k = 24
+    inits = [[0, 1, 2, 3, 4, 5] + list(rng.choice(np.arange(6, n), k - 6, replace=False)),
+             list(rng.choice(n, k, replace=False))]
+    for f64 in (False, True):
+        lab, cent, dist, it, inertia = kmeans_ensemble(
+            x, [k, k], inits, max_iter=4, centroid_mode="f64" if f64 else "numba")
+        for p in range(2):
+            rl, rc, ri = oracle.kmeans_fit(x, k, inits[p], max_iter=4, f64=f64)
+            assert np.array_equal(lab[p].cpu().numpy(), rl)
+            assert np.array_equal(cent[p].cpu().numpy(), rc)
+            assert int(it[p].item()) == ri
+
+
 def test_fit_empty_clusters_large_n(T):
     """Empty clusters with n above the one-thread limit of the quickselect:
     the block-parallel partition steps must reproduce the reference's
