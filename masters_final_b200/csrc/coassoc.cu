@@ -37,6 +37,8 @@
 
 #include <cuda_fp16.h>
 
+#include <algorithm>
+
 namespace eacb {
 
 constexpr int kMaxK = 8192;            // largest cluster id + 1 supported
@@ -67,6 +69,11 @@ constexpr int kNbrBytes = 64 * 1024;           // neighbourhood chunk: 524,288 c
 constexpr int kMaxGroupLists = 4096;           // (partition, cluster) lists per group
 constexpr int kNbrSmem = kNbrBytes + kMaxGroupLists * (8 + 8 + 4);
 constexpr int64_t kDenseRatioDefault = 16;
+// the count pass keeps each tile's pair counts (one byte per pair, 16 KB per
+// 128 x 128 tile) for the fill, in up to this many bytes per point (and at
+// most kPairBytesMax); a tile that finds no room is recomputed by the fill
+constexpr int64_t kPairBytesPerPoint = 8192;
+constexpr int64_t kPairBytesMax = (int64_t)32 << 30;
 
 // half2 words per point in the FP16 label copy: P rounded up to 8 partitions
 __host__ __device__ constexpr int32_t pair_words(int32_t P) { return ((P + 7) / 8) * 4; }
@@ -96,8 +103,11 @@ struct CoWS {
     unsigned long long *nbr_used;
     int32_t *rowlist;     // n: rows a streaming kernel takes
     int *rowlist_n;
+    uint8_t *pbuf;        // pair counts of the count pass's tiles, read by the fill
+    unsigned long long *pused;
+    int64_t *islot;       // per pair-tile item: its place in pbuf (-1: none)
     ScanScratch scan;
-    int64_t ntiles, nbr_cap;
+    int64_t ntiles, nbr_cap, pcap, nitems_max;
     int32_t Q;            // half2 words per point in lt
     static CoWS carve(Carver &c, int32_t n, int32_t P, int32_t K)
     {
@@ -106,6 +116,8 @@ struct CoWS {
         w.ntiles = ((int64_t)n + kMLTile - 1) / kMLTile;
         w.Q = pair_words(P);
         w.nbr_cap = 16 * (int64_t)n + 65536;
+        w.pcap = std::min<int64_t>(kPairBytesPerPoint * (int64_t)n + (1 << 20), kPairBytesMax);
+        w.nitems_max = (int64_t)n / kPT + K + 1;
         const int64_t pn = (int64_t)P * n;
         const int64_t m = (int64_t)P * K * w.ntiles;
         w.members = c.take<int32_t>(pn > 0 ? pn : 1);
@@ -130,6 +142,9 @@ struct CoWS {
         w.nbr_used = c.take<unsigned long long>(1);
         w.rowlist = c.take<int32_t>(n);
         w.rowlist_n = c.take<int>(1);
+        w.pbuf = c.take<uint8_t>(w.pcap);
+        w.pused = c.take<unsigned long long>(1);
+        w.islot = c.take<int64_t>(w.nitems_max);
         w.scan = ScanScratch::carve(c, m + 1 > n ? m + 1 : n, w.err);
         return w;
     }
@@ -704,6 +719,10 @@ struct PairCtx {
     const int *prow;
     int32_t n, K, Q;
     int64_t ntiles;
+    uint8_t *pbuf;            // kept pair counts (count pass writes, fill reads)
+    int64_t pcap;
+    unsigned long long *pused;
+    int64_t *islot;
 };
 
 // Column c of a tile sits at slot 8 (c % 16) + c / 16, so that the eight
@@ -748,6 +767,7 @@ k_pairs(PairCtx pc, TailCtx tc, const int32_t *order, const int64_t *cap_indptr,
     uint32_t *sC = psm + (size_t)Q * kPT;
     __shared__ int32_t s_row[kPT], s_col[kPT];
     __shared__ int64_t s_end[kPT], s_cur[kPT];
+    __shared__ int64_t s_slot;
     __shared__ int s_item, s_c0;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int pr = *pc.prow;
@@ -788,6 +808,20 @@ k_pairs(PairCtx pc, TailCtx tc, const int32_t *order, const int64_t *cap_indptr,
                 if (nb[m] > first) b = m; else a = m + 1;
             }
             s_c0 = a;
+            // the item's counts: a place reserved by the count pass, which
+            // the fill reads instead of comparing again
+            if (FILL) {
+                s_slot = pc.islot[t];
+            } else {
+                const int64_t need = (int64_t)((len - a + kPT - 1) / kPT) * kPairThreads * 64;
+                int64_t at = -1;
+                if (need > 0) {
+                    at = (int64_t)atomicAdd(pc.pused, (unsigned long long)need);
+                    if (at + need > pc.pcap) at = -1;
+                }
+                pc.islot[t] = at;
+                s_slot = at;
+            }
         }
         // this thread's rows: a row that takes no entries compares as INT_MAX
         int32_t ri[8];
@@ -801,33 +835,67 @@ k_pairs(PairCtx pc, TailCtx tc, const int32_t *order, const int64_t *cap_indptr,
             dcount[a] = 0;
         }
         __syncthreads();
-        for (int cb = s_c0; cb < len; cb += kPT) {
+        const int64_t slot = s_slot;
+        for (int cb = s_c0, ci = 0; cb < len; cb += kPT, ++ci) {
             for (int c = threadIdx.x; c < kPT; c += blockDim.x)
                 s_col[col_slot(c)] = cb + c < len ? nb[cb + c] : -1;
             __syncthreads();
-            load_pairs(sC, s_col, pc.lt, Q);
-            __syncthreads();
-            __half2 acc[8][8];
+            // the thread's 64 counts, one byte each: pw[2a + b/4] byte b%4 is
+            // (row 8ty + a, column tx + 16b)
+            uint32_t pw[16];
+            uint4 *kept = slot >= 0 ? reinterpret_cast<uint4 *>(
+                              pc.pbuf + slot + ((int64_t)ci * kPairThreads + threadIdx.x) * 64)
+                                    : nullptr;
+            if (FILL && slot >= 0) {
 #pragma unroll
-            for (int a = 0; a < 8; ++a)
-#pragma unroll
-                for (int b = 0; b < 8; ++b) acc[a][b] = __float2half2_rn(0.f);
-#pragma unroll 2
-            for (int w = 0; w < Q; ++w) {
-                const uint4 ra = *reinterpret_cast<const uint4 *>(sR + w * kPT + 8 * ty);
-                const uint4 rb = *reinterpret_cast<const uint4 *>(sR + w * kPT + 8 * ty + 4);
-                const uint4 ca = *reinterpret_cast<const uint4 *>(sC + w * kPT + 8 * tx);
-                const uint4 cc = *reinterpret_cast<const uint4 *>(sC + w * kPT + 8 * tx + 4);
-                const uint32_t R[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
-                const uint32_t C[8] = {ca.x, ca.y, ca.z, ca.w, cc.x, cc.y, cc.z, cc.w};
-#pragma unroll
-                for (int a = 0; a < 8; ++a) {
-                    const __half2 rv = *reinterpret_cast<const __half2 *>(&R[a]);
-#pragma unroll
-                    for (int b = 0; b < 8; ++b)
-                        acc[a][b] = __hadd2(acc[a][b],
-                                            __heq2(rv, *reinterpret_cast<const __half2 *>(&C[b])));
+                for (int q = 0; q < 4; ++q) {
+                    const uint4 v = kept[q];
+                    pw[4 * q] = v.x;
+                    pw[4 * q + 1] = v.y;
+                    pw[4 * q + 2] = v.z;
+                    pw[4 * q + 3] = v.w;
                 }
+            } else {
+                load_pairs(sC, s_col, pc.lt, Q);
+                __syncthreads();
+                __half2 acc[8][8];
+#pragma unroll
+                for (int a = 0; a < 8; ++a)
+#pragma unroll
+                    for (int b = 0; b < 8; ++b) acc[a][b] = __float2half2_rn(0.f);
+#pragma unroll 2
+                for (int w = 0; w < Q; ++w) {
+                    const uint4 ra = *reinterpret_cast<const uint4 *>(sR + w * kPT + 8 * ty);
+                    const uint4 rb = *reinterpret_cast<const uint4 *>(sR + w * kPT + 8 * ty + 4);
+                    const uint4 ca = *reinterpret_cast<const uint4 *>(sC + w * kPT + 8 * tx);
+                    const uint4 cc = *reinterpret_cast<const uint4 *>(sC + w * kPT + 8 * tx + 4);
+                    const uint32_t R[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
+                    const uint32_t C[8] = {ca.x, ca.y, ca.z, ca.w, cc.x, cc.y, cc.z, cc.w};
+#pragma unroll
+                    for (int a = 0; a < 8; ++a) {
+                        const __half2 rv = *reinterpret_cast<const __half2 *>(&R[a]);
+#pragma unroll
+                        for (int b = 0; b < 8; ++b)
+                            acc[a][b] = __hadd2(
+                                acc[a][b], __heq2(rv, *reinterpret_cast<const __half2 *>(&C[b])));
+                    }
+                }
+#pragma unroll
+                for (int a = 0; a < 8; ++a)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        uint32_t word = 0;
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            const __half2 v = acc[a][4 * h + e];
+                            word |= (uint32_t)(__low2float(v) + __high2float(v)) << (8 * e);
+                        }
+                        pw[2 * a + h] = word;
+                    }
+                if (!FILL && slot >= 0)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        kept[q] = make_uint4(pw[4 * q], pw[4 * q + 1], pw[4 * q + 2], pw[4 * q + 3]);
             }
             int32_t cj[8];
 #pragma unroll
@@ -842,7 +910,7 @@ k_pairs(PairCtx pc, TailCtx tc, const int32_t *order, const int64_t *cap_indptr,
                 const int64_t end = FILL ? s_end[8 * ty + a] : 0;
 #pragma unroll
                 for (int b = 0; b < 8; ++b) {
-                    const int cnt = (int)(__low2float(acc[a][b]) + __high2float(acc[a][b]));
+                    const int cnt = (int)((pw[2 * a + (b >> 2)] >> (8 * (b & 3))) & 255u);
                     const bool keep = cj[b] > ri[a] && cnt > 0;
                     if (FILL) {
                         const uint32_t m = (__ballot_sync(0xffffffffu, keep) >> half) & 0xffffu;
@@ -982,7 +1050,8 @@ static int launch_pairs(const CoWS &w, const TailCtx &tc, const int64_t *cap_ind
     if (smem > 200 * 1024) return EACB_ERR_UNSUPPORTED;
     EACB_CUDA(allow_max_dyn_smem(k_pairs<FILL>));
     PairCtx pc{w.lt, w.members, w.nbr, w.S, w.grp_off, w.grp_item0, w.grp_len, w.prow,
-               tc.n, tc.K, w.Q, w.ntiles};
+               tc.n, tc.K, w.Q, w.ntiles, w.pbuf, w.pcap, w.pused, w.islot};
+    if (!FILL) EACB_CUDA(cudaMemsetAsync(w.pused, 0, sizeof(unsigned long long), st));
     k_pairs<FILL><<<row_grid(2), kPairThreads, smem, st>>>(
         pc, tc, w.order, cap_indptr, indptr, w.rowcnt, w.rowflag, indices, data,
         &w.queue[FILL ? 6 : 5], w.maxcnt, w.err);
