@@ -4,8 +4,8 @@
 // products run as ONE BF16 GEMM with FP32 accumulation in tensor memory:
 // each float32 operand is split into three BF16 parts (h + m + l, ~24
 // significant bits) and the K dimension holds the six products that matter
-// (see put_row), the large h*h group last.  The epilogue (16 warps, one point
-// row per thread, a quarter of the columns per warp) reads the accumulator tile
+// (see put_row), the large h*h group last.  The epilogue (8 warps, one point
+// row per thread, half the columns per warp) reads the accumulator tile
 // from TMEM with tcgen05.ld, forms the screened distance and keeps the best
 // two per point.  A point whose runner-up lies within the proven error bound
 // E (|x|^2 + max|c|^2) of its winner (E from the split, the accumulation
@@ -14,13 +14,13 @@
 // reference distance.  Labels therefore equal the reference's
 // (MyML/MyML/cluster/KMeans.py:453-490) for any input.
 //
-// Shapes: M = 128 points per CTA, N <= 256 centroids per MMA tile, K = 6d
+// Shapes: M = 128 points per CTA, N <= 128 centroids per MMA tile, K = 6d
 // padded to a multiple of 16 (<= 192).  Operands are pre-arranged in global
 // memory in the UMMA K-major no-swizzle core-matrix layout (8 rows x 16
 // bytes per core matrix, LBO = 128 B along K, SBO = 128 B * K/8 along M/N),
 // so each tile is one contiguous cp.async.bulk copy into shared memory.
-// One thread issues the MMAs; TMEM holds one 128 x 256 FP32 accumulator per
-// CTA (256 columns), two CTAs per SM share the 512 columns and overlap each
+// One thread issues the MMAs; TMEM holds one 128 x 128 FP32 accumulator per
+// CTA (128 columns), four CTAs per SM share the 512 columns and overlap each
 // other's MMA and epilogue.  Every wait is bounded and reports an error.
 #include "kmeans_common.cuh"
 #include <cuda_bf16.h>
@@ -30,11 +30,11 @@
 namespace eacb {
 
 constexpr int kTM = 128;           // points per CTA tile
-constexpr int kTN = 256;           // centroids per MMA tile
-constexpr int kTThreads = 512;     // 16 warps: 4 TMEM lane quarters x 4 column quarters
+constexpr int kTN = 128;           // centroids per MMA tile
+constexpr int kTThreads = 256;     // 8 warps: 4 TMEM lane quarters x 2 column halves
 constexpr int kTColGroups = kTThreads / kTM;
 constexpr int kTColsPer = kTN / kTColGroups;
-constexpr int kTmemCols = 256;
+constexpr int kTmemCols = kTN;
 constexpr int kWaitLimit = 1 << 26;
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
@@ -247,7 +247,7 @@ __global__ void k_prep_centroids(const float *C, const int32_t *kk, int32_t kmax
 }
 
 // ---------------------------------------------------------------- labels --
-__global__ void __launch_bounds__(kTThreads, 2)
+__global__ void __launch_bounds__(kTThreads, 4)
 k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const float *__restrict__ C,
            const int32_t *__restrict__ kk, int32_t kmax, int32_t kt_max, int32_t P, int32_t ppc,
            const int32_t *__restrict__ active, const uint8_t *__restrict__ A,
@@ -312,7 +312,7 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
         bulk_g2s(sB[0], btile(p, 0), b_bytes, &bar_b[0]);
     }
     // epilogue ownership: row = 32*(warp%4) + lane (the TMEM lanes warp w may
-    // read), columns [64*(warp/4), +64)
+    // read), columns [64*(warp/4), +64) of the 128-column tile
     const int row = 32 * (warp & 3) + lane;
     const int cgrp = warp >> 2, colh = kTColsPer * cgrp;
     const int64_t i = tile0 * kTM + row;
@@ -406,7 +406,7 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
         __syncthreads();                         // the accumulator is free again
         if (s_fail) { ok = false; break; }
         if (t + 1 == tiles) {
-            // the partition is done: merge the column quarters of each row, in
+            // the partition is done: merge the column groups of each row, in
             // column order
             if (cgrp > 0) {
                 s_b1[cgrp - 1][row] = b1;
@@ -687,16 +687,17 @@ int label_pass_tc(const float *X, int32_t n, int32_t D, int32_t P, const float *
                            (16.0 * ((D + 15) / 16) + 4.0) * ldexp(1.0, -23);
     const float E = 2.f * (float)(dot_err + (D + 6) * ldexp(1.0, -24));
     const size_t a_bytes = (size_t)kTM * s.Kp * 2, b_bytes = (size_t)kTN * s.Kp * 2;
-    // CTAs per SM (two share the SM's 512 TMEM columns) and centroid tile
-    // buffers: tuning-table knobs; by default two CTAs, double-buffered while
-    // both still fit
-    const int ctas = tune_get(TUNE_TC_CTAS_PER_SM, D, n, 2) == 1 ? 1 : 2;
-    const size_t cap_bytes = ctas == 2 ? 110 * 1024 : 220 * 1024;
+    // CTAs per SM (each holds 128 TMEM columns): four by default, fewer when
+    // their operand tiles do not fit four to an SM
+    int ctas = (int)tune_get(TUNE_TC_CTAS_PER_SM, D, n, 4);
+    ctas = ctas >= 4 ? 4 : (ctas >= 2 ? 2 : 1);
+    while (ctas > 1 && a_bytes + b_bytes > (size_t)(220 / ctas) * 1024) ctas /= 2;
+    const size_t cap_bytes = (size_t)(220 / ctas) * 1024;
     int nbuf = (a_bytes + 2 * b_bytes <= cap_bytes) ? 2 : 1;
     nbuf = (int)std::min<int64_t>(nbuf, std::max<int64_t>(1, tune_get(TUNE_TC_BUFFERS, D, n, nbuf)));
     const size_t smem = a_bytes + nbuf * b_bytes;
     // a floor on the request so that no more CTAs than asked share an SM
-    const size_t floor_bytes = ctas == 2 ? 100 * 1024 : 120 * 1024;
+    const size_t floor_bytes = (size_t)(228 / (ctas + 1) + 2) * 1024;
     const size_t smem_req = smem < floor_bytes ? floor_bytes : smem;
     EACB_CUDA(allow_max_dyn_smem(k_label_tc));
     // one CTA per 128-point tile and share of the partitions: all partitions

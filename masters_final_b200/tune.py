@@ -13,9 +13,11 @@ tuned shapes.
 
 Knobs and the stage each one is timed on:
   tc_ctas_per_sm, tc_buffers   one batched K-Means fit of 4 partitions on the
-                               tensor-core labeler (per dimension d and n)
-  co_count_ctas, co_fill_ctas  the co-association count + fill of a
-                               20-partition label matrix (per n)
+                               tensor-core labeler (per dimension d and n;
+                               1, 2 or 4 CTAs per SM)
+  co_dense_ratio               the co-association build of a 20-partition
+                               K-Means ensemble (per n); the streaming
+                               passes' CTAs per SM keep their defaults
   mst_phase1_permille,         the Boruvka MST of the 16-NN graph of 1M points
   round_team (graph)
   round_team (EAC)             the final clustering of a co-association
@@ -93,7 +95,7 @@ def tune_kmeans(L, quick, out):
         ks = [int(k) for k in rng.integers(kr[0], kr[1], 4)]
         inits = [rng.choice(n, k, replace=False).tolist() for k in ks]
         a, b = (d, d), (n // 2, n * 2)
-        best, timings = _sweep(L, {"tc_ctas_per_sm": (a, b, (1, 2)), "tc_buffers": (a, b, (1, 2))},
+        best, timings = _sweep(L, {"tc_ctas_per_sm": (a, b, (1, 2, 4)), "tc_buffers": (a, b, (1, 2))},
                                lambda: _best_ms(lambda: kmeans_ensemble(
                                    X, ks, inits, max_iter=3, label_mode="bf16")), [])
         for k, v in best.items():
@@ -103,26 +105,34 @@ def tune_kmeans(L, quick, out):
 
 
 def tune_coassoc(L, quick, out):
+    """The pair tiles' work ratio (co_dense_ratio) on the co-association of a
+    20-partition K-Means ensemble of each workload's data (the choice only
+    moves groups between two exact paths)."""
+    import random as _random
+    from . import workloads as W
     from .EAC.sparse import CoassocBuilder, capacity_indptr
+    from .utils.partition import generate_ensemble_labels
     t = _lib.torch()
     for name, n, kr in COASSOC_SHAPES[:1] if quick else COASSOC_SHAPES:
-        rng = np.random.default_rng(3)
-        lab = np.stack([rng.integers(0, int(rng.integers(kr[0], kr[1])), n)
-                        for _ in range(20)]).astype(np.int32)
-        Ld = t.from_numpy(lab).cuda()
-        b0 = CoassocBuilder(Ld, n)
-        cap = capacity_indptr(n, b0.max_cluster * 3)
+        d, comps = (16, 50) if n <= 500_000 else (8, 200)
+        x = W.gaussian_mixture(n, d, comps, seed=3, sigma=1.0, center_range=20.0)
+        X = t.from_numpy(x).cuda()
+        np.random.seed(3)
+        _random.seed(3)
+        Ld, _ = generate_ensemble_labels(X, list(kr), 20, 3, label_mode="bf16")
+        del X
         a, b = (1, 255), (n // 2, n * 2)
 
         def run():
             bb = CoassocBuilder(Ld, n)
+            cap = capacity_indptr(n, bb.max_cluster * 3)
             return _best_ms(lambda: bb.build(cap), reps=2)
-        best, timings = _sweep(L, {"co_count_ctas": (a, b, (1, 2)),
-                                   "co_fill_ctas": (a, b, (1, 2))}, run, [])
+        best, timings = _sweep(L, {"co_dense_ratio": (a, b, (4, 16, 64))}, run, [])
         for k, v in best.items():
             out["entries"].append({"knob": k, "a": list(a), "b": list(b), "value": v,
-                                   "shape": name + " (20 partitions)", "timings": timings})
-        del Ld, b0
+                                   "shape": name + " (20 K-Means partitions)", "timings": timings})
+        del Ld
+        t.cuda.empty_cache()
 
 
 def tune_mst(L, quick, out):

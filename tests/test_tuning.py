@@ -52,8 +52,8 @@ def test_committed_table_loads():
         pytest.skip("no tuning table in this checkout")
     with open(_lib.TUNING_PATH) as f:
         table = json.load(f)
-    allowed = {"tc_ctas_per_sm": {1, 2}, "tc_buffers": {1, 2}, "co_count_ctas": {1, 2},
-               "co_fill_ctas": {1, 2}}
+    allowed = {"tc_ctas_per_sm": {1, 2, 4}, "tc_buffers": {1, 2}, "co_count_ctas": {1, 2},
+               "co_fill_ctas": {1, 2}, "co_dense_ratio": {4, 16, 64}}
     for e in table["entries"]:
         assert e["knob"] in _lib.TUNE_KNOBS
         assert e["a"][0] <= e["a"][1] and e["b"][0] <= e["b"][1]
