@@ -67,7 +67,9 @@ constexpr int kDenseMaxK = 2048;
 constexpr int kNbrThreads = 512;
 constexpr int kNbrBytes = 64 * 1024;           // neighbourhood chunk: 524,288 columns
 constexpr int kMaxGroupLists = 4096;           // (partition, cluster) lists per group
-constexpr int kNbrSmem = kNbrBytes + kMaxGroupLists * (8 + 8 + 4);
+// member positions fit 32 bits (P n < 2^31): cursors, ends and keys are
+// int32, so two CTAs fit an SM
+constexpr int kNbrSmem = kNbrBytes + kMaxGroupLists * (4 + 4 + 4);
 constexpr int64_t kDenseRatioDefault = 16;
 // the count pass keeps each tile's pair counts (one byte per pair, 16 KB per
 // 128 x 128 tile) for the fill, in up to this many bytes per point (and at
@@ -195,8 +197,8 @@ __device__ __forceinline__ int64_t block_sum(int64_t v)
 constexpr int kStreamU = 8;
 // Warps take tails dynamically (*next, zeroed by the caller before the
 // block's barrier), so warps that drew short tails take more of them.
-template <typename Op>
-__device__ __forceinline__ void stream_chunk(const int32_t *members, int64_t *ts, const int64_t *te,
+template <typename IT, typename Op>
+__device__ __forceinline__ void stream_chunk(const int32_t *members, IT *ts, const IT *te,
                                              int32_t P, int32_t jl, int *next, Op op)
 {
     const int lane = threadIdx.x & 31;
@@ -228,7 +230,7 @@ __device__ __forceinline__ void stream_chunk(const int32_t *members, int64_t *ts
             cur += taken;
             if (taken != kStreamU * 32) break;
         }
-        if (lane == 0) ts[p] = cur;
+        if (lane == 0) ts[p] = (IT)cur;
     }
 }
 
@@ -583,16 +585,15 @@ __device__ __forceinline__ int64_t first_above(const int32_t *members, int64_t a
 // One CTA per group (dynamic queue over the row-order partition's clusters):
 // the group's cluster lists, its rows' streaming cost, |N(g)| by chunked
 // bitmaps, the choice of path and, for the pair tiles, N(g) itself.
-__global__ void __launch_bounds__(kNbrThreads)
+__global__ void __launch_bounds__(kNbrThreads, 2)
 k_nbr(GroupCtx gc, int64_t ratio, int32_t *nbr, int64_t nbr_cap, unsigned long long *nbr_used,
       int64_t *grp_off, int32_t *grp_len, int32_t *grp_tiles, int32_t *rowflag, int *queue)
 {
     extern __shared__ __align__(16) uint8_t nsm[];
     uint32_t *bm = reinterpret_cast<uint32_t *>(nsm);
-    int64_t *ts = reinterpret_cast<int64_t *>(nsm + kNbrBytes);
-    int64_t *te = ts + kMaxGroupLists;
-    int32_t *cl = reinterpret_cast<int32_t *>(te + kMaxGroupLists);
-    __shared__ uint32_t lab[kDenseMaxK / 32];
+    int32_t *ts = reinterpret_cast<int32_t *>(nsm + kNbrBytes);
+    int32_t *te = ts + kMaxGroupLists;
+    int32_t *cl = te + kMaxGroupLists;
     __shared__ int s_g, s_nc, s_next, s_dense;
     __shared__ int64_t s_off;
     const int32_t n = gc.n, P = gc.P, K = gc.K;
@@ -610,30 +611,47 @@ k_nbr(GroupCtx gc, int64_t ratio, int32_t *nbr, int64_t nbr_cap, unsigned long l
         }
         const int32_t *rows = gc.members + gb;
         const int32_t lo = rows[0];
-        // 1. the clusters holding the group's rows, partition by partition
+        // 1. the clusters holding the group's rows, all partitions at once:
+        // bit p*K + c of a P x K bitmap, kept in the chunk bitmap's memory
+        // (unused until step 2; P*K <= 255 * 2048 bits fits its 64 KB); a
+        // thread takes a row through every partition, loads in flight
+        const int nwords = (int)(((int64_t)P * K + 31) >> 5);
         if (threadIdx.x == 0) s_nc = 0;
+        for (int w = threadIdx.x; w < nwords; w += blockDim.x) bm[w] = 0u;
+        __syncthreads();
+        // the streaming kernels' member visits for the group, estimated from
+        // at most 64 of its rows (it only chooses the path, never the result)
+        const int64_t vstep = size > 64 ? size / 64 : 1;
         int64_t visits = 0;
-        for (int p = 0; p < P; ++p) {
-            for (int w = threadIdx.x; w < (K + 31) / 32; w += blockDim.x) lab[w] = 0u;
-            __syncthreads();
-            for (int64_t t = threadIdx.x; t < size; t += blockDim.x) {
-                const int32_t i = rows[t];
+        for (int64_t t = threadIdx.x; t < size; t += blockDim.x) {
+            const int32_t i = rows[t];
+            const bool sample = t % vstep == 0 && t / vstep < 64;
+            const unsigned act = __activemask();
+            const int lane = threadIdx.x & 31;
+#pragma unroll 2
+            for (int p = 0; p < P; ++p) {
                 const int32_t c = gc.labels[(int64_t)p * n + i];
-                if (c >= 0 && c < K) {
-                    atomicOr(&lab[c >> 5], 1u << (c & 31));
+                const bool ok = c >= 0 && c < K;
+                // rows of a group mostly share a cluster: one atomic per
+                // distinct cluster of the warp
+                const unsigned peers = __match_any_sync(act, ok ? c : -1 - lane);
+                if (ok && lane == __ffs(peers) - 1) {
+                    const int bit = p * K + c;
+                    atomicOr(&bm[bit >> 5], 1u << (bit & 31));
+                }
+                if (ok && sample)
                     visits += gc.S[((int64_t)p * K + c + 1) * nt] -
                               gc.mypos[(int64_t)p * n + i] - 1;
-                }
             }
-            __syncthreads();
-            for (int w = threadIdx.x; w < (K + 31) / 32; w += blockDim.x)
-                for (uint32_t b = lab[w]; b; b &= b - 1u) {
-                    const int slot = atomicAdd(&s_nc, 1);
-                    if (slot < kMaxGroupLists) cl[slot] = p * K + w * 32 + __ffs(b) - 1;
-                }
-            __syncthreads();
         }
-        visits = block_sum<kNbrThreads>(visits);
+        __syncthreads();
+        for (int w = threadIdx.x; w < nwords; w += blockDim.x)
+            for (uint32_t b = bm[w]; b; b &= b - 1u) {
+                const int slot = atomicAdd(&s_nc, 1);
+                if (slot < kMaxGroupLists) cl[slot] = w * 32 + __ffs(b) - 1;
+            }
+        __syncthreads();
+        visits = block_sum<kNbrThreads>(visits) * vstep;
         const int nc = s_nc;
         bool dense = nc <= kMaxGroupLists;
         int64_t total = 0;
@@ -641,8 +659,8 @@ k_nbr(GroupCtx gc, int64_t ratio, int32_t *nbr, int64_t nbr_cap, unsigned long l
             // cursors: each list from its first member above the group's first row
             for (int e = threadIdx.x; e < nc; e += blockDim.x) {
                 const int64_t a = gc.S[(int64_t)cl[e] * nt], b = gc.S[((int64_t)cl[e] + 1) * nt];
-                ts[e] = first_above(gc.members, a, b, lo);
-                te[e] = b;
+                ts[e] = (int32_t)first_above(gc.members, a, b, lo);
+                te[e] = (int32_t)b;
             }
             __syncthreads();
             int64_t at = 0;
@@ -1112,7 +1130,7 @@ extern "C" int eacb_coassoc_prepare(const int32_t *labels, int32_t n, int32_t P,
         EACB_CUDA(cudaMemsetAsync(w.nbr_used, 0, sizeof(unsigned long long), st));
         EACB_CUDA(allow_max_dyn_smem(k_nbr));
         GroupCtx gc{labels, w.members, w.mypos, w.S, w.prow, n, P, K, w.Q, nt};
-        k_nbr<<<row_grid(1), kNbrThreads, kNbrSmem, st>>>(gc, ratio, w.nbr, w.nbr_cap, w.nbr_used,
+        k_nbr<<<row_grid(2), kNbrThreads, kNbrSmem, st>>>(gc, ratio, w.nbr, w.nbr_cap, w.nbr_used,
                                                           w.grp_off, w.grp_len, w.grp_tiles,
                                                           w.rowflag, &w.queue[4]);
         EACB_CHECK_LAUNCH();
