@@ -131,7 +131,7 @@ int eacb_scan_excl_i64(const int64_t *in, int64_t *out, int64_t n, int64_t init,
  * allocation, a plugin handed raw buffers and no allocator -- and so cannot
  * supply the workspace eacb_scan_excl_i32 needs.  Same inputs, outputs and
  * wrap-around as eacb_scan_excl_i32, no workspace argument: the look-back
- * scratch is a fixed array of about 512 KiB in the library's device image,
+ * scratch is a fixed array of about 350 KiB in the library's device image,
  * held on every GPU that loads the library until the process exits.  n may
  * not exceed EACB_SCAN_NOALLOC_MAX_N (returns EACB_ERR_WORKSPACE beyond it).
  * The first call on each device looks up that array's address

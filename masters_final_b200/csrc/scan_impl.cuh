@@ -5,7 +5,7 @@
 namespace eacb {
 
 constexpr int kScanThreads = 256;
-constexpr int kScanItems = 16;
+constexpr int kScanItems = 24;
 constexpr int64_t kScanTile = (int64_t)kScanThreads * kScanItems;
 
 struct ScanScratch {

@@ -10,7 +10,7 @@
 // How: the scan's look-back scratch (one status word per 4096-element tile,
 // a tile counter and an error word) lives in a fixed array in device memory,
 // defined below.  It is part of the library's image: every GPU that loads
-// libeacb200 holds it (about 512 KiB) until the process exits.  The device
+// libeacb200 holds it (about 350 KiB) until the process exits.  The device
 // address of that array is looked up once per device with
 // cudaGetSymbolAddress (a lookup, not an allocation), on the first call made
 // while that device is current; make that first call before any stream
@@ -28,7 +28,7 @@
 
 namespace {
 
-// n up to 2^28 elements -> 65,536 tiles of 4,096
+// n up to 2^28 elements -> 43,691 tiles of 6,144
 constexpr int64_t kNoAllocMaxN = EACB_SCAN_NOALLOC_MAX_N;
 constexpr int64_t kNoAllocTiles = kNoAllocMaxN / eacb::kScanTile + 1;
 // layout: [0] error word, [8..16) tile counter, [256..) tile status words
