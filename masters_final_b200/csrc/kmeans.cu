@@ -26,6 +26,8 @@
 #include "members.cuh"
 #include "kmeans_common.cuh"
 
+#include <type_traits>
+
 namespace eacb {
 
 constexpr int kLT = 128;         // label threads per block
@@ -256,6 +258,8 @@ k_inertia(const float *dists, int32_t n, int32_t P, int32_t *active, float *iner
 }
 
 // float32 (reference) or float64 sums of each cluster's members in point order
+constexpr int kCentDepth = 16;       // members in flight per lane
+
 template <bool F64>
 __global__ void k_centroids(const float *__restrict__ X, int32_t n, int32_t D,
                             const int32_t *__restrict__ members, const int64_t *__restrict__ S,
@@ -278,23 +282,36 @@ __global__ void k_centroids(const float *__restrict__ X, int32_t n, int32_t D,
         if (d == 0) atomicAdd(&nempty[p], 1);
         return;
     }
-    if (F64) {
-        double acc = 0.0;
-        for (int64_t m = s0; m < s1; ++m) acc += (double)X[(int64_t)members[m] * D + d];
-        *out = __double2float_rn(acc / (double)cnt);
-    } else {
-        float acc = 0.f;
-        int64_t m = s0;
-        for (; m + 4 <= s1; m += 4) {
-            const float v0 = X[(int64_t)members[m] * D + d];
-            const float v1 = X[(int64_t)members[m + 1] * D + d];
-            const float v2 = X[(int64_t)members[m + 2] * D + d];
-            const float v3 = X[(int64_t)members[m + 3] * D + d];
-            acc = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(acc, v0), v1), v2), v3);
+    // The sums are sequential in member order (the reference's order), so a
+    // cluster's sum is a chain as long as the cluster; the largest cluster
+    // sets the kernel's time.  Members go kCentDepth at a time: the next
+    // batch's ids load while this batch's coordinates do, and the adds follow
+    // in order, so a batch costs one memory latency.
+    using Acc = typename std::conditional<F64, double, float>::type;
+    Acc acc = 0;
+    auto add = [&](float v) {
+        if (F64) acc += (double)v;
+        else acc = (Acc)__fadd_rn((float)acc, v);
+    };
+    int64_t m = s0;
+    if (m + kCentDepth <= s1) {
+        int32_t id[kCentDepth];
+#pragma unroll
+        for (int q = 0; q < kCentDepth; ++q) id[q] = members[m + q];
+        for (; m + kCentDepth <= s1; m += kCentDepth) {
+            float v[kCentDepth];
+#pragma unroll
+            for (int q = 0; q < kCentDepth; ++q) v[q] = X[(int64_t)id[q] * D + d];
+            const bool more = m + 2 * kCentDepth <= s1;
+#pragma unroll
+            for (int q = 0; q < kCentDepth; ++q) id[q] = more ? members[m + kCentDepth + q] : 0;
+#pragma unroll
+            for (int q = 0; q < kCentDepth; ++q) add(v[q]);
         }
-        for (; m < s1; ++m) acc = __fadd_rn(acc, X[(int64_t)members[m] * D + d]);
-        *out = __double2float_rn(__ddiv_rn((double)acc, (double)cnt));
     }
+    for (; m < s1; ++m) add(X[(int64_t)members[m] * D + d]);
+    if (F64) *out = __double2float_rn((double)acc / (double)cnt);
+    else *out = __double2float_rn(__ddiv_rn((double)acc, (double)cnt));
 }
 
 // Empty clusters take the points arg_k_select returns for their number
