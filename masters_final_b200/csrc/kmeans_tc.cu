@@ -121,19 +121,23 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar)
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+// 32 accumulator columns of the warp's 32 TMEM lanes (one per thread)
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
 {
-    uint32_t r[16];
+    uint32_t r[32];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,"
+        "%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-          "=r"(r[14]), "=r"(r[15])
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 __host__ __device__ __forceinline__ uint32_t sbo_b(int Kp) { return 128u * (uint32_t)(Kp >> 3); }
@@ -378,12 +382,14 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
         tc_fence_after();
         const float *ncp = nc + ((int64_t)p * kt_max + t) * kTN;
         const int c_lo = colh, c_hi = min(colh + kTColsPer, nvalid);
-        for (int c0 = c_lo; c0 < c_hi; c0 += 16) {
-            float v[16], ncv[16];
-            tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c0, v);
-            // the 16 centroid norms, the same for every lane: four 16-byte loads
+        // 32 columns at a time (a 64-column share; past the tile's valid
+        // columns the norms are +inf, so those columns never win)
+        for (int c0 = c_lo; c0 < c_hi; c0 += 32) {
+            float v[32], ncv[32];
+            tmem_ld32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c0, v);
+            // the 32 centroid norms, the same for every lane: eight 16-byte loads
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < 8; ++q) {
                 const float4 f = __ldg(reinterpret_cast<const float4 *>(ncp + c0) + q);
                 ncv[4 * q] = f.x;
                 ncv[4 * q + 1] = f.y;
@@ -395,7 +401,7 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
             // one rounding, where adding |x|^2 first would take two
             const int cb = t * kTN + c0;
 #pragma unroll
-            for (int jj = 0; jj < 16; ++jj) {
+            for (int jj = 0; jj < 32; ++jj) {
                 const float sv = fmaf(-2.f, v[jj], ncv[jj]);      // ncp[c] = +inf past K
                 i1 = sv < b1 ? cb + jj : i1;
                 b2 = fminf(b2, fmaxf(b1, sv));
