@@ -436,10 +436,18 @@ k_label_tc(const float *__restrict__ X, int32_t n, int32_t D, int32_t Kp, const 
                         w2 = fminf(w2, o1);
                     }
                 }
-                // each screened distance is within E/2 (|x|^2 + max|c|^2) of
-                // the exact one (E carries a factor 2 of margin): the winner is
-                // certain when the runner-up is more than twice that above it
-                const float bound = E * (xn + cmax2[p]);
+                // Column c's screened distance is within e(c) = E/2 (|x|^2 +
+                // |c|^2) of the exact one.  A column c* that the exact
+                // arithmetic could rank at or before the winner w has
+                // |x - c*|^2 <= |x - c_w|^2 <= w1 + |x|^2 + e(w), so |c*| <=
+                // |x| + sqrt(w1 + |x|^2 + e(w)) (capped by the largest norm).
+                // The winner is certain when the runner-up is more than e(w) +
+                // e(c*) above it (the bound taken 1% wide for the rounding of
+                // this arithmetic).
+                const float ew = 0.5f * E * (xn + nc[((int64_t)p * kt_max) * kTN + wi]);
+                const float rc = sqrtf(xn) + sqrtf(fmaxf(0.f, w1 + xn + ew));
+                const float cstar2 = fminf(rc * rc, cmax2[p]);
+                const float bound = 1.01f * (ew + 0.5f * E * (xn + cstar2));
                 const int64_t o = (int64_t)p * n + i;
                 if (w2 - w1 > bound) {
                     float xv[32];
