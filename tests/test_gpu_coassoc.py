@@ -146,6 +146,29 @@ def test_coassoc_paths_vs_oracle(T, case, ratio):
     assert np.array_equal(c.data.cpu().numpy(), cnt)
 
 
+@pytest.mark.parametrize("ratio", [0, 10 ** 9])
+@pytest.mark.parametrize("n,P,k,holes", [(2, 1, 1, 0.0), (7, 3, 2, 0.0), (129, 1, 4, 0.0),
+                                         (130, 4, 3, 0.3), (257, 2, 1, 0.0), (300, 5, 40, 0.9)])
+def test_coassoc_paths_small_shapes(T, ratio, n, P, k, holes):
+    """Shapes at the edges of the pair tiles: fewer rows than one tile,
+    one row past a tile, a single partition, one cluster holding every
+    point, and mostly unlabelled points; both paths equal the oracle."""
+    from masters_final_b200 import _lib
+    rng = np.random.default_rng(n * 31 + P)
+    L = _random_labels(rng, P, n, k, k, holes)
+    ma = max(oracle.max_cluster_size(L), 1) * 3
+    cap = oracle.indptr_linear(n, ma)
+    ip, ind, cnt, nnz, disc, st = oracle.coassoc_build(L, cap)
+    if st != 0:
+        pytest.skip("the first partition overflows its capacity")
+    with _lib.forced("co_dense_ratio", ratio):
+        c = _build(L, n, ma)
+    assert c.nnz == nnz and c.nnz_discarded == disc
+    assert np.array_equal(c.indptr.cpu().numpy(), ip)
+    assert np.array_equal(c.indices.cpu().numpy(), ind)
+    assert np.array_equal(c.data.cpu().numpy(), cnt)
+
+
 @pytest.mark.parametrize("name", ["eac_small", "eac_discard", "eac_10k"])
 def test_coassoc_golden_pair_tiles(T, name):
     """The reference-run fixtures with every group on the pair tiles."""
