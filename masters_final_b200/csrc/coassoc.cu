@@ -31,6 +31,12 @@
 //     redone by a rank-aware kernel: a column's rank (first partition in
 //     processing order that associates it) is an atomicMin per visit, and
 //     the keep rule is applied from the rank histogram.
+//  4. the pair tiles (k_nbr, k_pairs): rows grouped by their
+//     cluster in the partition with the most clusters are counted by
+//     comparing label vectors over the group's neighbourhood instead of
+//     streaming tails, when that is cheaper; the count pass keeps each
+//     tile's pair counts for the fill.  Steps 2 and 3 then take only the
+//     rows outside those groups (and every row over its capacity).
 #include "eacb_common.cuh"
 #include "scan_impl.cuh"
 #include "members.cuh"
