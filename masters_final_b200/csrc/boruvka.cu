@@ -101,6 +101,16 @@ __device__ __forceinline__ void min_if_lower(unsigned long long *slot, uint64_t 
     if (v < __ldcg(slot)) atomicMin(slot, (unsigned long long)v);
 }
 
+// An offer that never waits: a reduction with no return value.  For kernels
+// whose slots each receive few offers (a graph's first phase: a vertex is
+// offered its incident edges only), where the check load of min_if_lower
+// would put an L2 round trip between consecutive offers of a thread.
+__device__ __forceinline__ void offer_min(unsigned long long *slot, uint64_t v, bool check)
+{
+    if (check) min_if_lower(slot, v);
+    else atomicMin(slot, (unsigned long long)v);
+}
+
 // One atomicMin per run of equal `su` among consecutive lanes.
 __device__ __forceinline__ void seg_min_atomic(bool valid, int32_t su, uint64_t sel,
                                                unsigned long long *best)
@@ -439,14 +449,70 @@ __device__ __forceinline__ bool phase_reserve(int64_t *s_cnt, unsigned long long
 
 // Graph rows are short (degrees), so a warp takes 32 consecutive rows per
 // block step, one row per lane for the row data.  When the 32 rows lie back
-// to back in the CSR (the usual layout), the warp walks their entries as one
-// flat range, 32 entries per step, each lane finding its entry's row among
-// the lanes' row starts (a 5-step shuffle search): the dependent loads of
-// all 32 rows overlap instead of running row after row.  Otherwise it walks
-// the rows one by one.  Kept words are staged in shared memory; the block
-// reserves once per step and copies them out coalesced (a warp whose
-// staging fills up flushes it on its own).
-constexpr int kPhStage = 512;            // staged words per warp
+// to back in the CSR (the usual layout) and their entries fit the warp's
+// row staging, the warp copies the whole range into shared memory with
+// coalesced 16-byte loads and each lane then walks its own row there: no
+// per-entry row search, and the row's own selection offer is one running
+// minimum in a register.  A longer back-to-back range is walked as one flat
+// range, 32 entries per step, each lane finding its entry's row among the
+// lanes' row starts (a 5-step shuffle search).  Otherwise the warp walks
+// the rows one by one.  Kept words are staged in shared memory.  In the
+// identity phase (every row read) the block reserves once per step and
+// copies them out coalesced; a later phase, which skips most rows, has no
+// block barrier: each warp flushes its staging when it fills up and at the
+// end.
+constexpr int kPhStage = 256;            // staged words per warp
+constexpr int kPhRowBytes = 3840;        // row staging per warp: entries x (4 + sizeof(WT))
+
+template <typename WT>
+struct RowCap {
+    static constexpr int value = (kPhRowBytes / (4 + (int)sizeof(WT))) & ~15;
+};
+
+// Copies entries [e_begin, e_end) of src (E entries) into the warp's dst and
+// returns the entry index that dst[0] holds: 16-byte vectors from the
+// aligned vector at or before e_begin when src is 16-byte aligned (every
+// vector read lies inside [0, E)), else one entry per lane.  The caller
+// checks that e_end - e_begin + 16 / sizeof(T) - 1 <= CAP.
+template <typename T, int CAP>
+__device__ __forceinline__ int64_t warp_copy_range(const T *src, int64_t e_begin, int64_t e_end,
+                                                   int64_t E, T *dst)
+{
+    constexpr int VEC = 16 / (int)sizeof(T);
+    constexpr int NV = (CAP / VEC + 31) / 32;      // vectors per lane at most
+    constexpr int NB = 3;                          // vectors in flight per lane
+    const int lane = threadIdx.x & 31;
+    if (((uintptr_t)src & 15) == 0) {
+        const int64_t base = e_begin & ~(int64_t)(VEC - 1);
+        const int nv = (int)((e_end - base + VEC - 1) / VEC);
+#pragma unroll
+        for (int k0 = 0; k0 < NV; k0 += NB) {
+            if (lane + 32 * k0 >= nv) break;
+            uint4 x[NB];
+#pragma unroll
+            for (int k = 0; k < NB; ++k) {
+                const int i = lane + 32 * (k0 + k);
+                const int64_t e = base + (int64_t)i * VEC;
+                if (i < nv && e + VEC <= E) {
+                    x[k] = __ldg(reinterpret_cast<const uint4 *>(src + e));
+                } else {
+                    T t[VEC];
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) t[q] = (i < nv && e + q < E) ? src[e + q] : T(0);
+                    memcpy(&x[k], t, 16);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < NB; ++k) {
+                const int i = lane + 32 * (k0 + k);
+                if (i < nv) *reinterpret_cast<uint4 *>(dst + (int64_t)i * VEC) = x[k];
+            }
+        }
+        return base;
+    }
+    for (int64_t i = lane; i < e_end - e_begin; i += 32) dst[i] = src[e_begin + i];
+    return e_begin;
+}
 
 __device__ __forceinline__ void phase_flush_warp(const uint64_t *stage, int cnt, uint64_t *eout,
                                                  unsigned long long *cursor,
@@ -485,31 +551,37 @@ __device__ __forceinline__ void phase_stage(bool keep, uint64_t k, uint64_t *sta
 // identity: the first phase (every vertex its own root: no label is read,
 // and every entry is checked once for a destination out of range, and
 // counted into sym[0] (u < v) or sym[1] (u > v): a symmetric graph has as
-// many of each).
+// many of each).  Its selection offers are reductions with no check load: a
+// vertex is offered its own incident edges only.
 // skip_root (device int, or null; -1 = none): a later phase skips the rows of
 // that root -- the giant component the earlier phases built -- and emits
 // both directions of each kept entry whose other end lies in it, so the
 // giant still sees every edge it has to another component (each such edge is
 // found once, from the row outside the giant).
 template <int MODE, typename WT>
-__global__ void __launch_bounds__(kPhThreads)
+__global__ void __launch_bounds__(kPhThreads, 4)
 k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const WT *weight,
             int32_t V, int64_t E, int wbits, int lo, int hi, const int *dev_lohi, int slot,
             int identity, const int32_t *skip_root, const int32_t *label, Pack pk,
             uint64_t *eout, unsigned long long *cursor, unsigned long long cap,
             unsigned long long *best, unsigned long long *sym, int *err)
 {
-    unsigned long long n_lt = 0, n_gt = 0;   // this lane's entries by direction
+    unsigned n_lt = 0, n_gt = 0;             // this lane's entries by direction (the warp sum is 32-bit)
     if (dev_lohi) {
         lo = dev_lohi[2 * slot];
         hi = dev_lohi[2 * slot + 1];
     }
     const int32_t skip = skip_root ? *skip_root : -1;
+    constexpr int kCap = RowCap<WT>::value;
     __shared__ uint64_t stage_all[kPhWarps][kPhStage];
+    __shared__ __align__(16) int32_t rdest_all[kPhWarps][kCap];
+    __shared__ __align__(16) WT rw_all[kPhWarps][kCap];
     __shared__ int64_t s_cnt[kPhWarps];
     __shared__ unsigned long long s_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint64_t *stage = stage_all[warp];
+    int32_t *rdest = rdest_all[warp];
+    WT *rw = rw_all[warp];
     const int64_t step = (int64_t)kPhWarps * 32;
     auto root_of = [&](int32_t v) -> int32_t { return identity ? v : label[v]; };
     // a kept entry u -> v (roots lu != lv) becomes one word for the
@@ -522,20 +594,30 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
         const uint64_t k = keep ? pk.make(w, (uint32_t)u, (uint32_t)v) : 0ull;
         phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
         if (keep) {
-            min_if_lower(&best[lu],
-                         MODE == SEL_MST ? (k >> 1) : (((uint64_t)w << 32) | (uint32_t)lv));
-            min_if_lower(&best[lv],
-                         MODE == SEL_MST ? (k >> 1) : (((uint64_t)w << 32) | (uint32_t)lu));
+            offer_min(&best[lu], MODE == SEL_MST ? (k >> 1) : (((uint64_t)w << 32) | (uint32_t)lv),
+                      !identity);
+            offer_min(&best[lv], MODE == SEL_MST ? (k >> 1) : (((uint64_t)w << 32) | (uint32_t)lu),
+                      !identity);
         }
     };
+    int cnt = 0;                         // staged words (carried across steps without identity)
+    // the next step's row labels are loaded one step ahead (a later phase
+    // spends most steps on this load alone: its rows are mostly skipped)
+    auto row_label = [&](int64_t r) -> int32_t {
+        const int64_t u = r + (int64_t)warp * 32 + lane;
+        return (identity || u >= V) ? (int32_t)u : label[u];
+    };
+    int32_t lu_next = row_label((int64_t)blockIdx.x * step);
     for (int64_t r0 = (int64_t)blockIdx.x * step; r0 < V; r0 += (int64_t)gridDim.x * step) {
         const int64_t u0 = r0 + (int64_t)warp * 32;
         const int nrows = u0 >= V ? 0 : (int)(V - u0 < 32 ? V - u0 : 32);
         int64_t f = 0, d = 0;
         int32_t lu = 0;
         bool live = false;
+        const int32_t lu_this = lu_next;
+        lu_next = row_label(r0 + (int64_t)gridDim.x * step);
         if (lane < nrows) {
-            lu = root_of((int32_t)(u0 + lane));
+            lu = lu_this;
             live = lu != skip;
             if (live) {
                 f = first[u0 + lane];
@@ -547,7 +629,6 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
                 }
             }
         }
-        int cnt = 0;
         if (__any_sync(0xffffffffu, live)) {
             // rows back to back?  (row l + 1 starts where row l ends; a
             // skipped row must not break the range, so it counts as empty
@@ -561,7 +642,51 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
             const int64_t e_end = __shfl_sync(0xffffffffu, f + d, llast);
             const bool flat = __all_sync(0xffffffffu, linked) && lmask == (nrows >= 32 ? 0xffffffffu : ((1u << nrows) - 1u)) &&
                               e_end - e_begin < ((int64_t)1 << 30);
-            if (flat) {
+            // the whole range fits the row staging (with the slack of the
+            // aligned first vector of either array)
+            constexpr int kSlack = 16 / (int)(sizeof(WT) < 4 ? sizeof(WT) : 4) - 1;
+            if (flat && e_end - e_begin + kSlack <= kCap) {
+                const int64_t db = warp_copy_range<int32_t, kCap>(dest, e_begin, e_end, E, rdest);
+                const int64_t wb = warp_copy_range<WT, kCap>(weight, e_begin, e_end, E, rw);
+                __syncwarp();
+                const int32_t od = (int32_t)(f - db), ow = (int32_t)(f - wb);
+                const int32_t u = (int32_t)(u0 + lane);
+                const int dl = (int)d;                  // 0 past the last row
+                const int dmax = (int)__reduce_max_sync(0xffffffffu, (unsigned)dl);
+                uint64_t mine = kNone;                  // this row's own offer
+                for (int j = 0; j < dmax; ++j) {
+                    bool cand = false;
+                    int32_t v = -1;
+                    uint32_t w = 0;
+                    if (j < dl) {
+                        v = rdest[od + j];
+                        w = wword(rw[ow + j]);
+                        if (v < 0 || v >= V) {
+                            set_err(err, DEV_BAD_INPUT);
+                        } else if (v != u) {
+                            if (v > u) ++n_lt; else ++n_gt;
+                            const int bk = (int)wbucket(w, wbits);
+                            cand = bk > lo && bk <= hi;
+                        }
+                    }
+                    const int32_t lv = cand ? root_of(v) : 0;
+                    // the same words and offers as emit(): one word per
+                    // undirected edge, offered to both ends
+                    const bool keep = cand && lv != lu && (u < v || lv == skip);
+                    const uint64_t k = keep ? pk.make(w, (uint32_t)u, (uint32_t)v) : 0ull;
+                    phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
+                    if (keep) {
+                        const uint64_t su = MODE == SEL_MST ? (k >> 1)
+                                                            : (((uint64_t)w << 32) | (uint32_t)lv);
+                        mine = su < mine ? su : mine;
+                        offer_min(&best[lv],
+                                  MODE == SEL_MST ? (k >> 1) : (((uint64_t)w << 32) | (uint32_t)lu),
+                                  !identity);
+                    }
+                }
+                if (mine != kNone) offer_min(&best[lu], mine, !identity);
+                __syncwarp();                           // the row staging is reused
+            } else if (flat) {
                 const int32_t frel = (int32_t)(f - e_begin);      // row starts, warp-relative
                 // four 32-entry slices per step, the loads of all in flight together
                 constexpr int S = 4;
@@ -639,20 +764,29 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
                 }
             }
         }
-        if (lane == 0) s_cnt[warp] = cnt;
-        const bool fits = phase_reserve(s_cnt, &s_base, cursor, 1, cap, err);
-        if (fits) {
-            const unsigned long long at = s_base + (unsigned long long)s_cnt[warp];
-            for (int i = lane; i < cnt; i += 32) eout[at + i] = stage[i];
+        if (identity) {
+            // identity is uniform over the grid, so every thread of the
+            // block takes the reservation's barriers
+            if (lane == 0) s_cnt[warp] = cnt;
+            const bool fits = phase_reserve(s_cnt, &s_base, cursor, 1, cap, err);
+            if (fits) {
+                const unsigned long long at = s_base + (unsigned long long)s_cnt[warp];
+                for (int i = lane; i < cnt; i += 32) eout[at + i] = stage[i];
+            }
+            __syncthreads();      // staging and s_cnt are reused by the next step
+            cnt = 0;
         }
-        __syncthreads();          // staging and s_cnt are reused by the next step
+    }
+    if (!identity && cnt > 0) {
+        __syncwarp();
+        phase_flush_warp(stage, cnt, eout, cursor, cap, err);
     }
     if (sym) {
         n_lt = __reduce_add_sync(0xffffffffu, (unsigned)n_lt);
         n_gt = __reduce_add_sync(0xffffffffu, (unsigned)n_gt);
         if ((threadIdx.x & 31) == 0 && (n_lt | n_gt)) {
-            atomicAdd(&sym[0], n_lt);
-            atomicAdd(&sym[1], n_gt);
+            atomicAdd(&sym[0], (unsigned long long)n_lt);
+            atomicAdd(&sym[1], (unsigned long long)n_gt);
         }
     }
 }
@@ -1662,17 +1796,21 @@ __global__ void k_key2eid(const uint64_t *keys, int64_t n_keys, const int32_t *f
         const uint32_t w = pk.sel_w(s);
         const int64_t f = first[a], d = deg[a];
         int64_t found = -1;
-        for (int64_t e0 = f; e0 < f + d && found < 0; e0 += 4) {
-            int32_t v[4];
-            uint32_t ww[4];
+        // the first 16 entries in one batch of loads (most rows of a k-NN
+        // graph end there), the rest 8 at a time
+        for (int64_t e0 = f; e0 < f + d && found < 0; e0 += (e0 == f ? 16 : 8)) {
+            int32_t v[16];
+            uint32_t ww[16];
+            const int span = e0 == f ? 16 : 8;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
+            for (int i = 0; i < 16; ++i) {
                 const int64_t e = e0 + i;
-                v[i] = e < f + d ? dest[e] : -1;
-                ww[i] = e < f + d ? wword(weight[e]) : 0u;
+                const bool in = i < span && e < f + d;
+                v[i] = in ? dest[e] : -1;
+                ww[i] = in ? wword(weight[e]) : 0u;
             }
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < 16; ++i)
                 if (found < 0 && v[i] == b && ww[i] == w) found = e0 + i;
         }
         if (found < 0) set_err(err, DEV_BAD_INPUT);   // graph not symmetric
