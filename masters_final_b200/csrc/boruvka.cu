@@ -1107,24 +1107,6 @@ __global__ void k_phase_plan(const unsigned long long *hist, int *lohi, int p1_p
     }
 }
 
-__global__ void k_iota(int32_t *a, int64_t n)
-{
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x)
-        a[i] = (int32_t)i;
-}
-
-// Every vertex its own root (parent) and its own successor (color): a root
-// that no round visits keeps color[s] == s.
-__global__ void k_iota2(int32_t *a, int32_t *b, int64_t n)
-{
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        a[i] = (int32_t)i;
-        b[i] = (int32_t)i;
-    }
-}
-
 constexpr int kMaxRounds = 96;   // Boruvka rounds per phase (halving: 96 is never reached)
 
 // Round state kept on the device (int64 words), so that the phases of an MST
@@ -1145,25 +1127,6 @@ enum : int {
     C_COUNT = 16
 };
 
-// Start of a phase queued without a host read: its edge count is the
-// build's cursor, its supervertex count the previous phase's result (V0 for
-// the first phase).
-__global__ void k_phase_begin(int64_t *cnt, int64_t V0, int first_phase)
-{
-    if (threadIdx.x == 0) {
-        if (first_phase) cnt[C_V] = V0;
-        cnt[C_E] = cnt[C_CURSOR];
-    }
-}
-
-__global__ void k_set_sizes(int64_t *cnt, int64_t V, int64_t E)
-{
-    if (threadIdx.x == 0) {
-        cnt[C_V] = V;
-        cnt[C_E] = E;
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Boruvka rounds: all rounds of a phase in ONE persistent kernel.
 //
@@ -1180,8 +1143,8 @@ __global__ void k_set_sizes(int64_t *cnt, int64_t V, int64_t E)
 // Each participant owns a contiguous chunk of the original vertices (its
 // part of the active list) and a contiguous segment of the phase's edge
 // words; both shrink in place.  Between the steps of a round the
-// participants meet at a barrier: a bounded spin on a generation word for the
-// grid, __syncthreads for one block.  Once few active roots and edges are
+// participants meet at a barrier: a bounded spin on an arrival counter for
+// the grid, __syncthreads for one block.  Once few active roots and edges are
 // left, the grid's other blocks leave and block 0 runs the remaining rounds
 // alone for every participant's chunk and segment (no grid barriers).
 // A round is
@@ -1224,49 +1187,48 @@ constexpr int64_t kSoloEdges = 8192;
 constexpr int kFindLimit = 1 << 20;             // parent-chain steps (a forest is shorter)
 
 struct GridBarrier {
-    unsigned count;
-    unsigned gen;
+    unsigned count;       // arrivals since the launch began (never reset inside one)
+    unsigned pad;
 };
 
-// Grid-wide barrier of a cooperative launch.  Thread 0 of each block arrives
-// on a counter; the last to arrive resets it and advances the generation the
-// others wait on.  The wait gives up after about a second (DEV_SPIN_LIMIT),
-// or as soon as any block has raised an error, so a block that left early
-// never holds the others.  Returns false when it gave up.  The fences order
-// each block's writes before its arrival and its reads after the wait; the
-// data exchanged between blocks is read with L1-bypassing loads.
-__device__ __forceinline__ bool grid_barrier(GridBarrier *b, int *err)
+// Grid-wide barrier of a cooperative launch.  Thread 0 of each block adds
+// its arrival to a counter that only grows, with no return value, and waits
+// until the counter reaches (barriers passed + 1) x blocks: no block resets
+// anything, so the last arrival is the only write the others wait for.  The
+// counter starts at zero (the host clears it before each launch).  The wait
+// gives up after about a second (DEV_SPIN_LIMIT), or as soon as any block
+// has raised an error, so a block that left early never holds the others.
+// Returns false when it gave up.  The fences order each block's writes
+// before its arrival and its reads after the wait; the data exchanged between
+// blocks is read with L1-bypassing loads.
+__device__ __forceinline__ bool grid_barrier(GridBarrier *b, unsigned &passed, int *err)
 {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned *vgen = &b->gen;
-        const unsigned g = *vgen;
+        const unsigned target = (passed + 1u) * gridDim.x;
+        volatile unsigned *vc = &b->count;
         __threadfence();
+        atomicAdd(&b->count, 1u);
         int ok = 1;
-        if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
-            atomicExch(&b->count, 0u);
-            __threadfence();
-            atomicAdd(&b->gen, 1u);
-        } else {
-            long long spins = 0;
-            while (*vgen == g) {
-                if (*(volatile int *)err) {
-                    ok = 0;
-                    break;
-                }
-                if (++spins > kBarrierSpins) {
-                    set_err(err, DEV_SPIN_LIMIT);
-                    ok = 0;
-                    break;
-                }
-                if (spins > 256) __nanosleep(32);
+        long long spins = 0;
+        while ((int)(*vc - target) < 0) {
+            if (*(volatile int *)err) {
+                ok = 0;
+                break;
             }
+            if (++spins > kBarrierSpins) {
+                set_err(err, DEV_SPIN_LIMIT);
+                ok = 0;
+                break;
+            }
+            if (spins > 256) __nanosleep(32);
         }
         __threadfence();
         s_ok = ok;
     }
     __syncthreads();
+    ++passed;
     return s_ok != 0;
 }
 
@@ -1287,6 +1249,8 @@ struct RoundArgs {
     GridBarrier *bar;
     int *err;
     int max_rounds;
+    int from_cursor;              // edge count = cnt[C_CURSOR] (a queued phase's build)
+    int first_phase;              // supervertex count = V0
 };
 
 // Roots of N vertices at once (all parent loads of one level issued
@@ -1378,12 +1342,16 @@ k_rounds(RoundArgs a)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     bool solo = !GRID;                  // one block does all the work
     int64_t Pe = P;                     // participants whose chunks and segments are in use
+    unsigned passed = 0;                // grid barriers passed (the same in every block)
     auto sync = [&]() -> bool {
-        if (!solo) return grid_barrier(a.bar, a.err);
+        if (!solo) return grid_barrier(a.bar, passed, a.err);
         __syncthreads();
         return true;
     };
-    int64_t V = __ldcg(a.cnt + C_V), E = __ldcg(a.cnt + C_E);
+    // a queued weight phase starts from its build's cursor and the previous
+    // phase's supervertex count (V0 for the first phase)
+    int64_t V = a.first_phase ? a.V0 : __ldcg(a.cnt + C_V);
+    int64_t E = __ldcg(a.cnt + (a.from_cursor ? C_CURSOR : C_E));
     int64_t nmst = __ldcg(a.cnt + C_NMST);
     const int64_t E0 = E;
     const int64_t seg_stride = (E0 + P - 1) / P;     // edge segment of participant q
@@ -1701,19 +1669,60 @@ k_rounds(RoundArgs a)
 
 // Points every original vertex at its root (the next phase's builds and the
 // final labels read roots directly).
-__global__ void k_flatten(int32_t *parent, int64_t V0, int *err)
+// With next_best set, it also readies the next weight phase of a queued MST:
+// every selection slot empty, the build cursor and the round kernel's barrier
+// at zero (the round kernel that precedes it has ended).
+__global__ void k_flatten(int32_t *parent, int64_t V0, int *err, unsigned long long *next_best,
+                          int64_t *cnt, GridBarrier *bar)
 {
+    if (next_best && blockIdx.x == 0 && threadIdx.x == 0) {
+        cnt[C_CURSOR] = 0;
+        bar->count = 0;
+    }
     const int64_t stride = (int64_t)gridDim.x * blockDim.x * 4;
     for (int64_t xb = (int64_t)blockIdx.x * blockDim.x * 4 + threadIdx.x; xb < V0; xb += stride) {
-        int32_t x[4], r[4];
+        int32_t r[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int64_t v = xb + (int64_t)i * blockDim.x;
-            x[i] = v < V0 ? (int32_t)v : -1;
-            r[i] = x[i];
+            r[i] = v < V0 ? (int32_t)v : -1;
+            if (next_best && v < V0) next_best[v] = kNone;
         }
         find_batch<4>(parent, r, err);
-        (void)x;
+    }
+}
+
+// Engine state for a new run: no error, the round state, weight histogram
+// and barrier at zero, every selection slot empty, and every vertex its own
+// root (parent) and its own successor (color; a root that no round visits
+// keeps color[s] == s).
+__global__ void k_engine_reset(int *err, int64_t *cnt, unsigned long long *hist, GridBarrier *bar,
+                               unsigned long long *best, int32_t *parent, int32_t *color,
+                               int64_t n)
+{
+    if (blockIdx.x == 0) {
+        if (threadIdx.x == 0) {
+            *err = 0;
+            bar->count = 0;
+        }
+        for (int i = threadIdx.x; i < C_COUNT; i += blockDim.x) cnt[i] = 0;
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0ull;
+    }
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        best[i] = kNone;
+        parent[i] = (int32_t)i;
+        color[i] = (int32_t)i;
+    }
+}
+
+// Sizes of a round-kernel run started from the host, and its barrier at zero.
+__global__ void k_set_sizes(int64_t *cnt, int64_t V, int64_t E, GridBarrier *bar)
+{
+    if (threadIdx.x == 0) {
+        cnt[C_V] = V;
+        cnt[C_E] = E;
+        bar->count = 0;
     }
 }
 
@@ -1890,20 +1899,22 @@ struct Engine {
 
     int reset(cudaStream_t st)
     {
-        EACB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
-        EACB_CUDA(cudaMemsetAsync(cnt, 0, C_COUNT * sizeof(int64_t), st));
-        EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V0, st));
-        k_iota2<<<grid_for(V0, 256), 256, 0, st>>>(label, color, V0);
+        k_engine_reset<<<grid_for(V0, 256), 256, 0, st>>>(err, cnt, hist, bar, best, label, color,
+                                                         V0);
         EACB_CHECK_LAUNCH();
         return EACB_OK;
     }
 
-    // Runs the rounds of one phase: input edges in ea (cnt[C_E] of them),
-    // supervertices [0, cnt[C_V]) with their selection in best.  One launch;
-    // with profiling on it is timed, and its algorithmic bytes come from the
-    // per-round sizes the kernel records.
+    // Runs the rounds of one phase: input edges in ea (cnt[C_E] of them, or
+    // cnt[C_CURSOR] with from_cursor), supervertices [0, cnt[C_V]) (V0 with
+    // first_phase) with their selection in best; the barrier is at zero (the
+    // reset, k_set_sizes or the previous phase's k_flatten cleared it).  One
+    // launch; with profiling on it is timed, and its algorithmic bytes come
+    // from the per-round sizes the kernel records.  With next_phase set, the
+    // flattening after it readies the next queued phase.
     template <int MODE>
-    int rounds(Pack pk, cudaStream_t st, int64_t e_hint)
+    int rounds(Pack pk, cudaStream_t st, int64_t e_hint, int from_cursor = 0,
+               int first_phase = 0, bool next_phase = false)
     {
         int team = 1;
         int s = round_team<MODE>(V0, e_hint, kind, &team);
@@ -1925,7 +1936,8 @@ struct Engine {
         a.bar = bar;
         a.err = err;
         a.max_rounds = g_round_cap > 0 ? std::min(g_round_cap, kMaxRounds) : kMaxRounds;
-        EACB_CUDA(cudaMemsetAsync(bar, 0, sizeof(GridBarrier), st));
+        a.from_cursor = from_cursor;
+        a.first_phase = first_phase;
         ProfScope ps(PROF_ROUNDS, st);
         if (team == 1) {
             k_rounds<MODE, false><<<1, kRT, 0, st>>>(a);
@@ -1954,30 +1966,30 @@ struct Engine {
             ps.done(bytes);
         }
         // every vertex to its root, for the next phase's builds and the labels
-        k_flatten<<<grid_for(V0, 256 * 4, 148 * 8), 256, 0, st>>>(label, V0, err);
+        k_flatten<<<grid_for(V0, 256 * 4, 148 * 8), 256, 0, st>>>(
+            label, V0, err, next_phase ? best : nullptr, cnt, bar);
         EACB_CHECK_LAUNCH();
         return EACB_OK;
     }
 
     // MST by weight phases (see k_phase_csr), all queued back to back with no
-    // host read in between: build(ph) appends a phase's edges to ea through
-    // cnt[C_CURSOR] with their selection in best; k_phase_begin turns the
-    // cursor into the round kernel's edge count.  One read at the end gives
-    // the forest size, the component count and any error.
+    // host read in between, right after reset(): build(ph) appends a phase's
+    // edges to ea through cnt[C_CURSOR] with their selection in best; the
+    // round kernel takes its edge count from the cursor, and the flattening
+    // after it clears the slots, the cursor and the barrier for the next
+    // phase.  One read at the end gives the forest size, the component count
+    // and any error.
     template <typename Build>
     int run_phased(Pack pk, const std::vector<Phase> &plan, Build build, cudaStream_t st,
                    int64_t *n_mst_out, int64_t *n_comp_out)
     {
         for (size_t q = 0; q < plan.size(); ++q) {
-            EACB_CUDA(cudaMemsetAsync(best, 0xff, sizeof(uint64_t) * V0, st));
-            EACB_CUDA(cudaMemsetAsync(&cnt[C_CURSOR], 0, sizeof(int64_t), st));
             Phase ph = plan[q];
             ph.ident = q == 0;                 // no round has merged anything yet
             int s = build(ph);
             if (s) return s;
-            k_phase_begin<<<1, 32, 0, st>>>(cnt, V0, q == 0 ? 1 : 0);
-            EACB_CHECK_LAUNCH();
-            if ((s = rounds<SEL_MST>(pk, st, Emax))) return s;
+            if ((s = rounds<SEL_MST>(pk, st, Emax, 1, q == 0 ? 1 : 0, q + 1 < plan.size())))
+                return s;
         }
         int64_t h[C_COUNT];
         int s = read_counts(st, h);
@@ -2079,7 +2091,7 @@ struct Engine {
     int run(Pack pk, int64_t E0, int64_t V_start, cudaStream_t st, int64_t *n_mst_total,
             int64_t *n_comp_out)
     {
-        k_set_sizes<<<1, 32, 0, st>>>(cnt, V_start, E0);
+        k_set_sizes<<<1, 32, 0, st>>>(cnt, V_start, E0, bar);
         EACB_CHECK_LAUNCH();
         int s = rounds<MODE>(pk, st, E0);
         if (s) return s;
@@ -2110,8 +2122,8 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
     const unsigned gr = grid_for((int64_t)V * 32, 256);
     const unsigned gph = grid_for(V, kPhThreads, 148 * 4);   // phase builds: grid-stride rows
     if (mode == SEL_MST) {
-        // weight phases over the bucket histogram of the entries
-        EACB_CUDA(cudaMemsetAsync(g.hist, 0, 256 * sizeof(unsigned long long), st));
+        // weight phases over the bucket histogram of the entries (the reset
+        // cleared it)
         if (E > 0) {
             if (sizeof(WT) == 1) {
                 if ((s = launch_whist_u8((const uint8_t *)weight, E, g.hist, st))) return s;
@@ -2519,7 +2531,7 @@ extern "C" int eacb_final_clustering(const int64_t *indptr, const int32_t *indic
     g.kind = 1;
     if ((s = g.reset(st))) return s;
     // 1. minimum spanning forest of the dissimilarity graph, by weight phases
-    EACB_CUDA(cudaMemsetAsync(g.hist, 0, 256 * sizeof(unsigned long long), st));
+    //    (the reset cleared the histogram)
     if (nnz > 0) {
         if ((s = launch_whist_u8(diassoc, nnz, g.hist, st))) return s;
     }
