@@ -6,7 +6,8 @@
 //
 // Design (not the reference's):
 //  * Every undirected edge is ONE 64-bit word: weight-order bits | min(u,v) |
-//    max(u,v) | 0, with u, v the ORIGINAL endpoints, offered to the selection
+//    max(u,v) | the entry's offset in the row of min(u,v) (graph MST; the
+//    spare bits) | direction, with u, v the ORIGINAL endpoints, offered to the selection
 //    slots of both its ends.  A round never rewrites edges; it only drops the
 //    ones that became internal.  The current endpoints are the roots of u
 //    and v in a union-find forest over the original vertices.
@@ -38,34 +39,50 @@ enum { SEL_MST = 0, SEL_CC = 1 };
 
 struct Pack {
     int vbits;
-    int wshift;      // 2*vbits + 1
+    int obits;       // row-offset bits (0: none)
+    int wshift;      // 2*vbits + obits + 1
     uint64_t vmask;
-    __host__ __device__ uint32_t a(uint64_t k) const { return (uint32_t)((k >> (vbits + 1)) & vmask); }
-    __host__ __device__ uint32_t b(uint64_t k) const { return (uint32_t)((k >> 1) & vmask); }
+    uint64_t omask;  // (1 << obits) - 1: also the "offset not recorded" value
+    __host__ __device__ uint32_t a(uint64_t k) const { return (uint32_t)((k >> (vbits + obits + 1)) & vmask); }
+    __host__ __device__ uint32_t b(uint64_t k) const { return (uint32_t)((k >> (obits + 1)) & vmask); }
     __host__ __device__ uint32_t w(uint64_t k) const { return (uint32_t)(k >> wshift); }
     __host__ __device__ uint32_t src(uint64_t k) const { return (k & 1) ? b(k) : a(k); }
     __host__ __device__ uint32_t dst(uint64_t k) const { return (k & 1) ? a(k) : b(k); }
-    __host__ __device__ uint64_t make(uint32_t w, uint32_t u, uint32_t v) const
+    // off: where the entry min -> max sits in the row of min (omask: not
+    // recorded); it is the lowest field of the selection key, so among
+    // parallel entries of one row the first one wins
+    __host__ __device__ uint64_t make(uint32_t w, uint32_t u, uint32_t v, uint64_t off) const
     {
         uint32_t lo = u < v ? u : v, hi = u < v ? v : u;
-        return ((uint64_t)w << wshift) | ((uint64_t)lo << (vbits + 1)) | ((uint64_t)hi << 1) |
-               (uint64_t)(u > v);
+        return ((uint64_t)w << wshift) | ((uint64_t)lo << (vbits + obits + 1)) |
+               ((uint64_t)hi << (obits + 1)) | ((off & omask) << 1) | (uint64_t)(u > v);
     }
-    // MST selection key (weight, min, max) and its decoding
+    __host__ __device__ uint64_t make(uint32_t w, uint32_t u, uint32_t v) const
+    {
+        return make(w, u, v, omask);
+    }
+    // MST selection key (weight, min, max, offset) and its decoding
     __host__ __device__ uint64_t mst_sel(uint64_t k) const { return k >> 1; }
-    __host__ __device__ uint32_t sel_a(uint64_t s) const { return (uint32_t)((s >> vbits) & vmask); }
-    __host__ __device__ uint32_t sel_b(uint64_t s) const { return (uint32_t)(s & vmask); }
-    __host__ __device__ uint32_t sel_w(uint64_t s) const { return (uint32_t)(s >> (2 * vbits)); }
+    __host__ __device__ uint32_t sel_a(uint64_t s) const { return (uint32_t)((s >> (vbits + obits)) & vmask); }
+    __host__ __device__ uint32_t sel_b(uint64_t s) const { return (uint32_t)((s >> obits) & vmask); }
+    __host__ __device__ uint32_t sel_w(uint64_t s) const { return (uint32_t)(s >> (2 * vbits + obits)); }
+    __host__ __device__ uint64_t sel_off(uint64_t s) const { return s & omask; }
 };
 
-static int make_pack(int32_t n_vertices, int wbits, Pack &pk)
+// with_offsets: the bits left over in the word hold the entry's row offset
+// (a graph MST returns entry ids: k_key2eid reads them instead of searching
+// the row).
+static int make_pack(int32_t n_vertices, int wbits, Pack &pk, bool with_offsets = false)
 {
     int vbits = 1;
     while (vbits < 31 && ((int64_t)1 << vbits) < (int64_t)n_vertices) vbits++;
     if (wbits + 2 * vbits + 1 > 64) return EACB_ERR_UNSUPPORTED;
+    const int spare = 64 - (wbits + 2 * vbits + 1);
     pk.vbits = vbits;
-    pk.wshift = 2 * vbits + 1;
+    pk.obits = with_offsets ? (spare < 24 ? spare : 24) : 0;
+    pk.wshift = 2 * vbits + pk.obits + 1;
     pk.vmask = ((uint64_t)1 << vbits) - 1;
+    pk.omask = ((uint64_t)1 << pk.obits) - 1;
     return EACB_OK;
 }
 
@@ -588,10 +605,14 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
     // undirected edge: written from the row of its smaller end, or from the
     // only row read when v lies in the skipped giant; its key is offered to
     // both ends (MST: (weight, min, max); CC: (weight, other end's root))
+    // (off: the entry's offset in row u, recorded when u is the smaller end)
     auto emit = [&](bool kept, uint32_t w, int32_t u, int32_t v, int32_t lu, int32_t lv,
-                    int &cnt) {
+                    int64_t off, int &cnt) {
         const bool keep = kept && (u < v || lv == skip);
-        const uint64_t k = keep ? pk.make(w, (uint32_t)u, (uint32_t)v) : 0ull;
+        const uint64_t k =
+            keep ? pk.make(w, (uint32_t)u, (uint32_t)v,
+                           (u < v && (uint64_t)off < pk.omask) ? (uint64_t)off : pk.omask)
+                 : 0ull;
         phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
         if (keep) {
             offer_min(&best[lu], MODE == SEL_MST ? (k >> 1) : (((uint64_t)w << 32) | (uint32_t)lv),
@@ -673,7 +694,10 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
                     // the same words and offers as emit(): one word per
                     // undirected edge, offered to both ends
                     const bool keep = cand && lv != lu && (u < v || lv == skip);
-                    const uint64_t k = keep ? pk.make(w, (uint32_t)u, (uint32_t)v) : 0ull;
+                    const uint64_t k =
+                        keep ? pk.make(w, (uint32_t)u, (uint32_t)v,
+                                       (u < v && (uint64_t)j < pk.omask) ? (uint64_t)j : pk.omask)
+                             : 0ull;
                     phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
                     if (keep) {
                         const uint64_t su = MODE == SEL_MST ? (k >> 1)
@@ -693,7 +717,7 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
                 for (int64_t e0 = e_begin; e0 < e_end; e0 += 32 * S) {
                     int64_t e[S];
                     int r[S];
-                    int32_t lr[S], v[S];
+                    int32_t lr[S], v[S], eo[S];
                     uint32_t w[S];
                     bool in[S];
 #pragma unroll
@@ -711,6 +735,7 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
                         }
                         r[q] = rr;
                         lr[q] = __shfl_sync(0xffffffffu, lu, rr);
+                        eo[q] = erel - __shfl_sync(0xffffffffu, frel, rr);   // offset in its row
                         v[q] = in[q] ? dest[e[q]] : -1;
                         w[q] = in[q] ? wword(weight[e[q]]) : 0u;
                     }
@@ -733,7 +758,7 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
 #pragma unroll
                     for (int q = 0; q < S; ++q)
                         emit(cand[q] && lv[q] != lr[q], w[q], (int32_t)(u0 + r[q]), v[q], lr[q],
-                             lv[q], cnt);
+                             lv[q], eo[q], cnt);
                 }
             } else {
                 for (int rr = 0; rr < nrows; ++rr) {
@@ -759,7 +784,7 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
                                 if (cand) lv = root_of(v);
                             }
                         }
-                        emit(cand && lv != lr, w, u, v, lr, lv, cnt);
+                        emit(cand && lv != lr, w, u, v, lr, lv, e - fr, cnt);
                     }
                 }
             }
@@ -1789,10 +1814,12 @@ static int round_team(int64_t V0, int64_t E, int kind, int *team)
 }
 
 // MST selection key -> index of its entry in row min(u,v) of a symmetric CSR
-// (the smallest index with the key's destination and weight).  One thread
-// per key scans the row, four entries per step with their loads in flight:
-// graph rows are short, and a thread per key keeps every key's dependent
-// loads (key -> row extent -> entries) overlapping with all the others.
+// (the smallest index with the key's destination and weight).  A key whose
+// build recorded the entry's offset in that row (the word's spare bits) is
+// one load of the row start.  Otherwise one thread per key scans the row,
+// with the loads of a step in flight together: graph rows are short, and a
+// thread per key keeps every key's dependent loads (key -> row extent ->
+// entries) overlapping with all the others.
 template <typename WT>
 __global__ void k_key2eid(const uint64_t *keys, int64_t n_keys, const int32_t *first,
                           const int32_t *deg, const int32_t *dest, const WT *weight, Pack pk,
@@ -1803,7 +1830,16 @@ __global__ void k_key2eid(const uint64_t *keys, int64_t n_keys, const int32_t *f
         const uint64_t s = keys[q];
         const int32_t a = (int32_t)pk.sel_a(s), b = (int32_t)pk.sel_b(s);
         const uint32_t w = pk.sel_w(s);
-        const int64_t f = first[a], d = deg[a];
+        const uint64_t off = pk.sel_off(s);
+        const int64_t f = first[a];
+        if (off != pk.omask) {
+            // the build recorded where the entry sits in row a: the first
+            // such entry, since a parallel entry of the row with a smaller
+            // offset has the smaller selection key
+            out[q] = (int32_t)(f + (int64_t)off);
+            continue;
+        }
+        const int64_t d = deg[a];
         int64_t found = -1;
         // the first 16 entries in one batch of loads (most rows of a k-NN
         // graph end there), the rest 8 at a time
@@ -2111,7 +2147,7 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
                          int64_t *host_n_comp, void *ws, size_t ws_bytes, cudaStream_t st)
 {
     Pack pk;
-    int s = make_pack(V, wbits, pk);
+    int s = make_pack(V, wbits, pk, mode == SEL_MST);
     if (s) return s;
     Carver c(ws, ws_bytes);
     Engine g = Engine::carve(c, V, E);
