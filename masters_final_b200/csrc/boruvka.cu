@@ -479,6 +479,9 @@ __device__ __forceinline__ bool phase_reserve(int64_t *s_cnt, unsigned long long
 // block barrier: each warp flushes its staging when it fills up and at the
 // end.
 constexpr int kPhStage = 256;            // staged words per warp
+constexpr int kPhChunk = 8;              // entries per row between dense passes
+constexpr int kPhRec = 32 * kPhChunk;    // kept-entry records per warp (dynamic shared memory)
+constexpr size_t kPhRecBytes = (size_t)kPhWarps * kPhRec * sizeof(int32_t);
 constexpr int kPhRowBytes = 3840;        // row staging per warp: entries x (4 + sizeof(WT))
 
 template <typename WT>
@@ -599,6 +602,8 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
     uint64_t *stage = stage_all[warp];
     int32_t *rdest = rdest_all[warp];
     WT *rw = rw_all[warp];
+    extern __shared__ int32_t ph_rec[];      // kPhWarps x kPhRec kept-entry records
+    int32_t *rec = ph_rec + warp * kPhRec;
     const int64_t step = (int64_t)kPhWarps * 32;
     auto root_of = [&](int32_t v) -> int32_t { return identity ? v : label[v]; };
     // a kept entry u -> v (roots lu != lv) becomes one word for the
@@ -674,41 +679,66 @@ k_phase_csr(const int32_t *first, const int32_t *deg, const int32_t *dest, const
                 const int32_t u = (int32_t)(u0 + lane);
                 const int dl = (int)d;                  // 0 past the last row
                 const int dmax = (int)__reduce_max_sync(0xffffffffu, (unsigned)dl);
-                uint64_t mine = kNone;                  // this row's own offer
-                for (int j = 0; j < dmax; ++j) {
-                    bool cand = false;
-                    int32_t v = -1;
-                    uint32_t w = 0;
-                    if (j < dl) {
-                        v = rdest[od + j];
-                        w = wword(rw[ow + j]);
-                        if (v < 0 || v >= V) {
-                            set_err(err, DEV_BAD_INPUT);
-                        } else if (v != u) {
-                            if (v > u) ++n_lt; else ++n_gt;
-                            const int bk = (int)wbucket(w, wbits);
-                            cand = bk > lo && bk <= hi;
+                const unsigned below = (1u << lane) - 1u;
+                // kPhChunk entries of every row at a time: a cheap test of
+                // each entry records the kept ones as (row lane, offset), then
+                // a dense pass over the records builds, stages and offers
+                // their words with every lane busy (a phase keeps a small
+                // share of the entries).  The same words and offers as
+                // emit(): one word per undirected edge, offered to both ends.
+                for (int j0 = 0; j0 < dmax; j0 += kPhChunk) {
+                    const int j1 = j0 + kPhChunk < dmax ? j0 + kPhChunk : dmax;
+                    int nrec = 0;
+                    for (int j = j0; j < j1; ++j) {
+                        bool keep = false;
+                        if (j < dl) {
+                            const int32_t v = rdest[od + j];
+                            if ((uint32_t)v >= (uint32_t)V) {
+                                set_err(err, DEV_BAD_INPUT);
+                            } else if (v != u) {
+                                if (v > u) ++n_lt; else ++n_gt;
+                                const int bk = (int)wbucket(wword(rw[ow + j]), wbits);
+                                if (bk > lo && bk <= hi) {
+                                    const int32_t lv = root_of(v);
+                                    keep = lv != lu && (u < v || lv == skip);
+                                }
+                            }
+                        }
+                        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                        if (keep) rec[nrec + __popc(bal & below)] = (lane << 16) | j;
+                        nrec += __popc(bal);
+                    }
+                    __syncwarp();
+                    for (int i0 = 0; i0 < nrec; i0 += 32) {
+                        const bool ok = i0 + lane < nrec;
+                        const int32_t rc = ok ? rec[i0 + lane] : 0;
+                        const int r = rc >> 16, jr = rc & 0xffff;
+                        const int32_t odr = __shfl_sync(0xffffffffu, od, r);
+                        const int32_t owr = __shfl_sync(0xffffffffu, ow, r);
+                        const int32_t lur = __shfl_sync(0xffffffffu, lu, r);
+                        const int32_t ur = (int32_t)(u0 + r);
+                        const int32_t v = ok ? rdest[odr + jr] : 0;
+                        const uint32_t w = ok ? wword(rw[owr + jr]) : 0u;
+                        const int32_t lv = ok ? root_of(v) : 0;
+                        const uint64_t k =
+                            ok ? pk.make(w, (uint32_t)ur, (uint32_t)v,
+                                         (ur < v && (uint64_t)jr < pk.omask) ? (uint64_t)jr
+                                                                             : pk.omask)
+                               : 0ull;
+                        phase_stage(ok, k, stage, cnt, eout, cursor, cap, err);
+                        if (ok) {
+                            offer_min(&best[lur],
+                                      MODE == SEL_MST ? (k >> 1)
+                                                      : (((uint64_t)w << 32) | (uint32_t)lv),
+                                      !identity);
+                            offer_min(&best[lv],
+                                      MODE == SEL_MST ? (k >> 1)
+                                                      : (((uint64_t)w << 32) | (uint32_t)lur),
+                                      !identity);
                         }
                     }
-                    const int32_t lv = cand ? root_of(v) : 0;
-                    // the same words and offers as emit(): one word per
-                    // undirected edge, offered to both ends
-                    const bool keep = cand && lv != lu && (u < v || lv == skip);
-                    const uint64_t k =
-                        keep ? pk.make(w, (uint32_t)u, (uint32_t)v,
-                                       (u < v && (uint64_t)j < pk.omask) ? (uint64_t)j : pk.omask)
-                             : 0ull;
-                    phase_stage(keep, k, stage, cnt, eout, cursor, cap, err);
-                    if (keep) {
-                        const uint64_t su = MODE == SEL_MST ? (k >> 1)
-                                                            : (((uint64_t)w << 32) | (uint32_t)lv);
-                        mine = su < mine ? su : mine;
-                        offer_min(&best[lv],
-                                  MODE == SEL_MST ? (k >> 1) : (((uint64_t)w << 32) | (uint32_t)lu),
-                                  !identity);
-                    }
+                    __syncwarp();                       // the records are reused
                 }
-                if (mine != kNone) offer_min(&best[lu], mine, !identity);
                 __syncwarp();                           // the row staging is reused
             } else if (flat) {
                 const int32_t frel = (int32_t)(f - e_begin);      // row starts, warp-relative
@@ -2189,7 +2219,11 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
             ProfScope ps(PROF_PHASE, st);
             // the first phase reads every row and needs many warps to keep
             // its loads in flight; the skipping phase touches few rows
-            k_phase_csr<SEL_MST, WT><<<ph.slot == 0 ? gr : gph, kPhThreads, 0, st>>>(
+            // the kept-entry records (dynamic) on top of the static staging pass 48 KB
+            EACB_CUDA(cudaFuncSetAttribute((const void *)k_phase_csr<SEL_MST, WT>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kPhRecBytes));
+            k_phase_csr<SEL_MST, WT><<<ph.slot == 0 ? gr : gph, kPhThreads, kPhRecBytes, st>>>(
                 first, deg, dest, weight, V, E, wbits, 0, 0, g.lohi, ph.slot, ph.slot == 0 ? 1 : 0,
                 ph.slot > 0 ? g.giant : nullptr, g.label, pk, g.ea,
                 (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best,
@@ -2205,7 +2239,10 @@ static int csr_graph_run(int mode, const int32_t *dest, const WT *weight, int wb
         // every entry with identity labels: one word per undirected edge and
         // each vertex's first selection (the reference's round one)
         if (E > 0) {
-            k_phase_csr<SEL_CC, WT><<<gr, kPhThreads, 0, st>>>(
+            EACB_CUDA(cudaFuncSetAttribute((const void *)k_phase_csr<SEL_CC, WT>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kPhRecBytes));
+            k_phase_csr<SEL_CC, WT><<<gr, kPhThreads, kPhRecBytes, st>>>(
                 first, deg, dest, weight, V, E, wbits, -1, 255, nullptr, 0, 1, nullptr, g.label, pk,
                 g.ea, (unsigned long long *)&g.cnt[C_CURSOR], (unsigned long long)g.Emax, g.best,
                 (unsigned long long *)&g.cnt[C_SYM_LT], g.err);
