@@ -1253,21 +1253,25 @@ struct GridBarrier {
 // counter starts at zero (the host clears it before each launch).  The wait
 // gives up after about a second (DEV_SPIN_LIMIT), or as soon as any block
 // has raised an error, so a block that left early never holds the others.
-// Returns false when it gave up.  The fences order each block's writes
-// before its arrival and its reads after the wait; the data exchanged between
-// blocks is read with L1-bypassing loads.
+// Returns false when it gave up.  The arrival is a release and the polling
+// load an acquire (gpu scope); with the block barriers around them they
+// order every thread's writes before the arrival and its reads after the
+// wait.  The data exchanged between blocks is read with L1-bypassing loads.
 __device__ __forceinline__ bool grid_barrier(GridBarrier *b, unsigned &passed, int *err)
 {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned target = (passed + 1u) * gridDim.x;
-        volatile unsigned *vc = &b->count;
-        __threadfence();
-        atomicAdd(&b->count, 1u);
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&b->count) : "memory");
+        auto count_now = [&]() -> unsigned {
+            unsigned c;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(&b->count) : "memory");
+            return c;
+        };
         int ok = 1;
         long long spins = 0;
-        while ((int)(*vc - target) < 0) {
+        while ((int)(count_now() - target) < 0) {
             if (*(volatile int *)err) {
                 ok = 0;
                 break;
@@ -1279,7 +1283,6 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier *b, unsigned &passed, i
             }
             if (spins > 256) __nanosleep(32);
         }
-        __threadfence();
         s_ok = ok;
     }
     __syncthreads();
@@ -1482,13 +1485,15 @@ k_rounds(RoundArgs a)
         // ---- B: forest edges, new roots, the next active list -----------
         int64_t merges = 0, epre = 0;           // all merges; forest edges before q0
         {
-            int64_t xp = 0, mg = 0;
+            // both below 2^31 (at most V0 each): one scan of (merges << 32) | edges
+            int64_t x = 0, tot = 0;
             for (int64_t j = tid; j < Pe; j += kRT) {
-                mg += __ldcg(a.part + kMaxTeam + j);
-                if (j < q0) xp += __ldcg(a.part + j);
+                x += (int64_t)__ldcg(a.part + kMaxTeam + j) << 32;
+                if (j < q0) x += __ldcg(a.part + j);
             }
-            block_excl_sum_shfl<kRT>(mg, merges);
-            block_excl_sum_shfl<kRT>(xp, epre);
+            block_excl_sum_shfl<kRT>(x, tot);
+            merges = tot >> 32;
+            epre = tot & 0xffffffffll;
         }
         for (int64_t q = q0; q < q1; ++q) {
             int32_t *al = a.act + vbase(q);
@@ -1649,16 +1654,18 @@ k_rounds(RoundArgs a)
         // ---- E: the next round's sizes, the same in every participant ----
         int64_t En = 0, An = 0;
         {
+            // the error flag is read beside the counts; the scans' block
+            // barriers publish s_err
+            const int e_now = tid == 0 ? *(volatile int *)a.err : 0;
             int64_t x = 0, y = 0;
             for (int64_t j = tid; j < Pe; j += kRT) {
                 x += __ldcg(a.seg + j);
                 y += __ldcg(a.alen + j);
             }
+            if (tid == 0) s_err = e_now;
             block_excl_sum_shfl<kRT>(x, En);
             block_excl_sum_shfl<kRT>(y, An);
         }
-        if (tid == 0) s_err = *(volatile int *)a.err;
-        __syncthreads();
         if (p == 0 && tid == 0 && round < kMaxRounds) {
             a.trace[3 * round] = V;
             a.trace[3 * round + 1] = E;
