@@ -1685,31 +1685,72 @@ k_rounds(RoundArgs a)
             // every block decides alike: the others leave, and block 0 moves
             // all active roots and edge words to the front of its own chunk
             // and segment, in participant order (list order = id order is
-            // kept).  A destination never passes its source, so tiles are
-            // copied forward, each read before it is written.
+            // kept).  The participants' counts are read at once and their
+            // exclusive prefixes kept in shared memory; the copy then runs
+            // over the concatenated elements, kRT at a time, each element
+            // finding its participant by binary search.  A destination never
+            // passes its source, so each chunk is read before it is written.
             solo = true;
             if (p != 0) return;
-            int64_t ao = 0, eo = 0;
-            for (int64_t q = 0; q < Pe; ++q) {
-                const int64_t n = __ldcg(a.alen + q), m = __ldcg(a.seg + q);
-                const int32_t *asrc = a.act + vbase(q);
-                const uint64_t *esrc = a.e + ebase(q);
-                for (int64_t j = 0; j < n; j += kRT) {
-                    const int32_t v = j + tid < n ? __ldcg(asrc + j + tid) : 0;
-                    __syncthreads();
-                    if (j + tid < n) a.act[ao + j + tid] = v;
-                    __syncthreads();
+            static_assert(2 * kRT >= kMaxTeam, "two participants per thread");
+            __shared__ int64_t s_apre[kMaxTeam + 1], s_epre[kMaxTeam + 1];
+            {
+                const int64_t j0 = 2 * (int64_t)tid;
+                const int64_t a0 = j0 < Pe ? (int64_t)__ldcg(a.alen + j0) : 0;
+                const int64_t a1 = j0 + 1 < Pe ? (int64_t)__ldcg(a.alen + j0 + 1) : 0;
+                const int64_t m0 = j0 < Pe ? __ldcg(a.seg + j0) : 0;
+                const int64_t m1 = j0 + 1 < Pe ? __ldcg(a.seg + j0 + 1) : 0;
+                int64_t at, mt;
+                const int64_t ax = block_excl_sum_shfl<kRT>(a0 + a1, at);
+                const int64_t mx = block_excl_sum_shfl<kRT>(m0 + m1, mt);
+                if (j0 < Pe) {
+                    s_apre[j0] = ax;
+                    s_epre[j0] = mx;
                 }
-                for (int64_t j = 0; j < m; j += kRT) {
-                    const uint64_t v = j + tid < m ? __ldcg(esrc + j + tid) : 0ull;
-                    __syncthreads();
-                    if (j + tid < m) a.e[eo + j + tid] = v;
-                    __syncthreads();
+                if (j0 + 1 < Pe) {
+                    s_apre[j0 + 1] = ax + a0;
+                    s_epre[j0 + 1] = mx + m0;
                 }
-                ao += n;
-                eo += m;
+                if (tid == 0) {
+                    s_apre[Pe] = at;
+                    s_epre[Pe] = mt;
+                }
             }
             __syncthreads();
+            const int64_t ao = s_apre[Pe], eo = s_epre[Pe];
+            // the participant holding concatenated element i: the last q < Pe
+            // with pre[q] <= i (pre[0] = 0)
+            auto owner = [&](const int64_t *pre, int64_t i) -> int64_t {
+                int64_t lo = 0, hi = Pe - 1;
+                while (lo < hi) {
+                    const int64_t mid = (lo + hi + 1) >> 1;
+                    if (pre[mid] <= i) lo = mid;
+                    else hi = mid - 1;
+                }
+                return lo;
+            };
+            for (int64_t c = 0; c < ao; c += kRT) {
+                const int64_t i = c + tid;
+                int32_t v = 0;
+                if (i < ao) {
+                    const int64_t q = owner(s_apre, i);
+                    v = __ldcg(a.act + vbase(q) + (i - s_apre[q]));
+                }
+                __syncthreads();
+                if (i < ao) a.act[i] = v;
+                __syncthreads();
+            }
+            for (int64_t c = 0; c < eo; c += kRT) {
+                const int64_t i = c + tid;
+                uint64_t v = 0;
+                if (i < eo) {
+                    const int64_t q = owner(s_epre, i);
+                    v = __ldcg(a.e + ebase(q) + (i - s_epre[q]));
+                }
+                __syncthreads();
+                if (i < eo) a.e[i] = v;
+                __syncthreads();
+            }
             if (tid == 0) {
                 a.alen[0] = (int32_t)ao;
                 a.seg[0] = eo;
