@@ -1418,16 +1418,33 @@ k_rounds(RoundArgs a)
     auto vbase = [&](int64_t q) { return min(a.V0, q * vchunk); };
 
     // ---- active list: the roots with a selection, in id order -------------
+    // (kRV consecutive vertices per thread: the loads of all in flight, one
+    // block scan per kRT * kRV vertices)
     for (int64_t q = solo ? 0 : p; q < (solo ? P : p + 1); ++q) {
         const int64_t v0 = vbase(q), v1 = min(a.V0, v0 + vchunk);
         int64_t kept = 0;
-        for (int64_t xb = v0; xb < v1; xb += kRT) {
-            const int64_t x = xb + tid;
-            const bool in = x < v1;
-            const bool on = in && __ldcg(a.parent + x) == (int32_t)x && __ldcg(a.best + x) != kNone;
+        for (int64_t xb = v0; xb < v1; xb += (int64_t)kRT * kRV) {
+            const int64_t x0 = xb + (int64_t)tid * kRV;
+            int32_t par[kRV];
+            uint64_t sel[kRV];
+#pragma unroll
+            for (int i = 0; i < kRV; ++i) {
+                const bool in = x0 + i < v1;
+                par[i] = in ? __ldcg(a.parent + x0 + i) : -1;
+                sel[i] = in ? __ldcg(a.best + x0 + i) : kNone;
+            }
+            int c = 0;
+            bool on[kRV];
+#pragma unroll
+            for (int i = 0; i < kRV; ++i) {
+                on[i] = par[i] == (int32_t)(x0 + i) && sel[i] != kNone;
+                c += on[i] ? 1 : 0;
+            }
             int64_t ttot;
-            const int64_t ex = block_excl_sum_shfl<kRT>(on ? 1 : 0, ttot);
-            if (on) a.act[v0 + kept + ex] = (int32_t)x;
+            int64_t at = v0 + kept + block_excl_sum_shfl<kRT>(c, ttot);
+#pragma unroll
+            for (int i = 0; i < kRV; ++i)
+                if (on[i]) a.act[at++] = (int32_t)(x0 + i);
             kept += ttot;
         }
         const int64_t e0 = ebase(q);
