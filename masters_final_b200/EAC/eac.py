@@ -42,7 +42,7 @@ def sp_sl_lifetime_csr(indptr, indices, diassoc, n, max_dist, n_clusters=0,
         lab = labels
     if returnDevAry:
         return int(nf.value), lab
-    return int(nf.value), lab.cpu().numpy()
+    return int(nf.value), _lib.to_host(lab)
 
 
 def sp_sl_lifetime(mat, max_dist=None, n_clusters=0):

@@ -290,6 +290,21 @@ def to_device(a, dtype=None):
     return x.to(device(), non_blocking=False).contiguous()
 
 
+def to_host(x):
+    """CUDA tensor -> numpy array through a pinned host buffer (torch's
+    caching host allocator): the copy runs at the link's speed instead of
+    being staged through pageable memory, and the array is a view that
+    keeps the buffer alive.  Copies on the current stream and waits for it
+    (the library's calls have finished their own stream by then)."""
+    t = torch()
+    if x.numel() == 0:
+        return np.empty(tuple(x.shape), dtype=np_dtype_of(x))
+    h = t.empty(tuple(x.shape), dtype=x.dtype, pin_memory=True)
+    h.copy_(x.contiguous(), non_blocking=True)
+    t.cuda.current_stream(x.device).synchronize()
+    return h.numpy()
+
+
 def np_dtype_of(x):
     t = torch()
     if isinstance(x, t.Tensor):

@@ -32,7 +32,7 @@ def connected_comps_gpu(dest, weight, firstEdge, outDegree, MAX_TPB=512, stream=
                "connected_comps_gpu")
     if returnDevAry:
         return labels
-    return labels.cpu().numpy()
+    return _lib.to_host(labels)
 
 
 connected_comps_seq = connected_comps_gpu

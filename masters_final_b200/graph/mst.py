@@ -7,8 +7,6 @@ are those of the unique forest under the order (weight, min(u,v), max(u,v)).
 """
 import ctypes
 
-import numpy as np
-
 from .. import _lib
 
 
@@ -41,9 +39,8 @@ def boruvka_minho_gpu(dest, weight, firstEdge, outDegree, MAX_TPB=512, stream=No
     n = int(n.value)
     if returnDevAry:
         return mst, n
-    out = np.empty(max(V - 1, 0), dtype=np.int32)
-    out[:n] = mst[:n].cpu().numpy()
-    return out, n
+    # V - 1 entries, the first n of them the forest (the reference's shape)
+    return _lib.to_host(mst[:max(V - 1, 0)]), n
 
 
 # The reference ships a CPU twin with the same contract
