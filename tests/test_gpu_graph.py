@@ -163,6 +163,101 @@ def test_boruvka_weight_types(T, dt):
     _check_mst(ip, d, w, mst, n)
 
 
+def _layout_permuted(indptr, dest, w, seed):
+    """The same rows stored in a random order, 0-2 junk entries before each
+    (first / deg point at each row's new place): no warp of 32 consecutive
+    vertices finds its rows back to back."""
+    V = indptr.size - 1
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(V)
+    deg = np.diff(indptr).astype(np.int32)
+    gaps = rng.integers(0, 3, V)
+    starts = np.concatenate([[0], np.cumsum(deg[order] + gaps)])
+    d2 = np.zeros(int(starts[-1]), np.int32)
+    w2 = np.full(int(starts[-1]), 255, w.dtype)
+    first = np.empty(V, np.int32)
+    for pos, u in enumerate(order):
+        f = int(starts[pos] + gaps[pos])
+        first[u] = f
+        d2[f:f + deg[u]] = dest[indptr[u]:indptr[u + 1]]
+        w2[f:f + deg[u]] = w[indptr[u]:indptr[u + 1]]
+    return first, deg, d2, w2
+
+
+def _with_parallel(indptr, dest, w, seed):
+    """5% of the undirected edges get a second entry at the end of both
+    rows: half with the same weight (the first entry stays the one an MST
+    returns), half one lighter (the new entry becomes it)."""
+    V = indptr.size - 1
+    rng = np.random.default_rng(seed)
+    ua, ub, uw = oracle.upper_edges(indptr, dest, w)
+    pick = rng.choice(ua.size, ua.size // 20, replace=False)
+    rows = [list(zip(dest[indptr[u]:indptr[u + 1]].tolist(), w[indptr[u]:indptr[u + 1]].tolist()))
+            for u in range(V)]
+    for j, i in enumerate(pick):
+        a, b, x = int(ua[i]), int(ub[i]), int(uw[i])
+        x2 = x if (j % 2 == 0 or x == 0) else x - 1
+        rows[a].append((b, x2))
+        rows[b].append((a, x2))
+    deg = np.array([len(r) for r in rows], np.int32)
+    ip = np.concatenate([[0], np.cumsum(deg)]).astype(np.int64)
+    d2 = np.array([e[0] for r in rows for e in r], np.int32)
+    w2 = np.array([e[1] for r in rows for e in r], w.dtype)
+    return ip[:-1].astype(np.int32), deg, d2, w2
+
+
+def _check_layout(first, deg, dest, w, mst, n):
+    """MST ids on any row layout: each is the first entry of row min(u,v)
+    with its destination and weight, and the forest (as pairs, and its total
+    weight) is the oracle Kruskal forest.  Returns the canonical CSR."""
+    V = first.size
+    rows = np.full(dest.size, -1, np.int64)
+    for u in range(V):
+        rows[first[u]:first[u] + deg[u]] = u
+    ids = mst[:n].astype(np.int64)
+    a, b = rows[ids], dest[ids].astype(np.int64)
+    assert np.all(a >= 0) and np.all(a < b)
+    for e, u, v in zip(ids.tolist(), a.tolist(), b.tolist()):
+        seg = slice(int(first[u]), e)
+        assert not np.any((dest[seg] == v) & (w[seg] == w[e]))
+    indptr = np.concatenate([[0], np.cumsum(deg)]).astype(np.int64)
+    take = np.concatenate([np.arange(first[u], first[u] + deg[u]) for u in range(V)])
+    cd, cw = dest[take], w[take]
+    ua, ub, uw = oracle.upper_edges(indptr, cd, cw)
+    f = oracle.kruskal_forest(V, ua, ub, uw)
+    assert n == f.sum()
+    assert set(zip(a.tolist(), b.tolist())) == set(zip(ua[f].tolist(), ub[f].tolist()))
+    assert w[ids].astype(np.int64).sum() == uw[f].astype(np.int64).sum()
+    return indptr, cd, cw
+
+
+def _layout_case(layout):
+    from masters_final_b200 import workloads as W
+    if layout == "high_degree":
+        indptr, dest, w = W.knn_graph(20000, k=48, seed=33)
+        return indptr[:-1].astype(np.int32), np.diff(indptr).astype(np.int32), dest, w
+    indptr, dest, w = W.knn_graph(20000, k=16, seed=31)
+    if layout == "parallel":
+        return _with_parallel(indptr, dest, w, 32)
+    return _layout_permuted(indptr, dest, w, 34)
+
+
+@pytest.mark.parametrize("layout", ["permuted", "parallel", "high_degree"])
+def test_boruvka_csr_layouts(T, layout):
+    """Rows out of order with gaps (the row-by-row build), parallel entries
+    (the recorded row offsets must still name the first matching entry) and
+    rows too long for a warp's row staging (the flat walk): the forest, its
+    entry ids and the component labels against the oracle."""
+    from masters_final_b200.graph.mst import boruvka_minho_gpu
+    from masters_final_b200.graph.connected_components import connected_comps_gpu
+    first, deg, dest, w = _layout_case(layout)
+    mst, n = boruvka_minho_gpu(dest, w, first, deg)
+    indptr, cd, cw = _check_layout(first, deg, dest, w, mst, n)
+    labels = connected_comps_gpu(dest, w, first, deg)
+    _, ref = oracle.boruvka_seq(indptr, cd, cw)
+    assert np.array_equal(labels, ref)
+
+
 def test_final_clustering_golden(T):
     from masters_final_b200.EAC.eac import sp_sl_lifetime_csr
     for name in ("eac_small", "eac_discard"):
