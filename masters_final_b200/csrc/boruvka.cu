@@ -427,10 +427,10 @@ static int launch_whist_u8(const uint8_t *w, int64_t n, unsigned long long *hist
 
 // Phase builds: the edges of a weight-bucket range (lo, hi] whose endpoints
 // are in different components, appended to eout, with the first round's
-// minimum-edge selection.  The rows of a block step reserve their output
-// slots with one atomicAdd, which keeps the shared cursor off the critical
-// path.  Edge order is not deterministic, results are: selection uses a
-// strict total order.
+// minimum-edge selection.  Output slots are reserved with one atomicAdd per
+// block step (the identity phase) or per warp staging flush, which keeps the
+// shared cursor off the critical path.  Edge order is not deterministic,
+// results are: selection uses a strict total order.
 // the final clustering merges its remaining weight phases once fewer than
 // one component per this many points is left
 constexpr int64_t kMergeBelow = 64;
@@ -468,9 +468,10 @@ __device__ __forceinline__ bool phase_reserve(int64_t *s_cnt, unsigned long long
 // block step, one row per lane for the row data.  When the 32 rows lie back
 // to back in the CSR (the usual layout) and their entries fit the warp's
 // row staging, the warp copies the whole range into shared memory with
-// coalesced 16-byte loads and each lane then walks its own row there: no
-// per-entry row search, and the row's own selection offer is one running
-// minimum in a register.  A longer back-to-back range is walked as one flat
+// coalesced 16-byte loads and each lane then walks its own row there, with
+// no per-entry row search: an inexpensive test records the kept entries,
+// and a dense pass builds and offers their words (see kPhChunk).  A longer
+// back-to-back range is walked as one flat
 // range, 32 entries per step, each lane finding its entry's row among the
 // lanes' row starts (a 5-step shuffle search).  Otherwise the warp walks
 // the rows one by one.  Kept words are staged in shared memory.  In the
