@@ -82,3 +82,13 @@ def test_dense_path_not_built():
     e = EAC(10, sparse=False)
     with pytest.raises(NotImplementedError):
         e.buildMatrix(np.zeros((2, 10), dtype=np.int32))
+
+
+def test_to_host_empty_result():
+    """An empty device result (the final clustering when no labels are
+    produced) comes back as an empty array of the same dtype without
+    touching the device or the pinned allocator."""
+    import torch
+    from masters_final_b200 import _lib
+    out = _lib.to_host(torch.empty(0, dtype=torch.int32))
+    assert isinstance(out, np.ndarray) and out.dtype == np.int32 and out.shape == (0,)
